@@ -1,0 +1,131 @@
+"""ctypes binding of libcgc.so (the C ABI declared in include/cgc.h).
+
+The library is the only compute path: if it is missing or cannot be loaded,
+every call raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcgc.so")
+
+CGC_OK = 0
+ERRORS = {
+    1: "CGC_ERR_ARG", 2: "CGC_ERR_OOM", 3: "CGC_ERR_CUDA", 4: "CGC_ERR_TIMEOUT",
+    5: "CGC_ERR_NOT_CONVERGED", 6: "CGC_ERR_OVERFLOW", 7: "CGC_ERR_STATE",
+    8: "CGC_ERR_NOT_GRID", 9: "CGC_ERR_NO_DEVICE",
+}
+SEG_SINK_REACH = 0
+SEG_SOURCE_MIN = 1
+SCHED_PARITY = 0
+SCHED_ASYNC = 1
+
+
+class CgcError(RuntimeError):
+    """Raised for a non-zero status of a cgc_* call (mirrors the reference's
+    ExceptionBase thrown by CUGIP_CHECK_RESULT, include/cugip/exception.hpp:33-47)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [("struct_size", C.c_int32), ("local_pulses", C.c_int32), ("sweeps_per_relabel", C.c_int32),
+                ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
+                ("reserved", C.c_int32 * 10)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("flow", C.c_int64), ("sweeps", C.c_int64), ("global_relabels", C.c_int64),
+                ("bfs_rounds", C.c_int64), ("tiles_swept", C.c_int64), ("tiles_relabelled", C.c_int64),
+                ("pulses", C.c_int64), ("solve_ms", C.c_double), ("kernel_ms", C.c_double),
+                ("launches", C.c_int64), ("reserved", C.c_int64 * 6)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class VolumeSpec(C.Structure):
+    _fields_ = [("X", C.c_int32), ("Y", C.c_int32), ("Z", C.c_int32), ("kind", C.c_int32),
+                ("seed", C.c_uint64), ("count", C.c_int32), ("n_fixed_radii", C.c_int32),
+                ("fixed_radii", C.c_double * 8), ("radius_min", C.c_double), ("radius_max", C.c_double),
+                ("intensity_min", C.c_double), ("intensity_max", C.c_double), ("background", C.c_double),
+                ("noise_sd", C.c_double), ("mu_bg", C.c_double), ("mu_fg", C.c_double), ("class_sd", C.c_double),
+                ("tlink_scale", C.c_double), ("nlink_scale", C.c_double), ("nlink_sigma", C.c_double),
+                ("ctrl_min", C.c_int32), ("ctrl_max", C.c_int32), ("edge_sigma", C.c_double)]
+
+
+P32 = C.POINTER(C.c_int32)
+PU32 = C.POINTER(C.c_uint32)
+PU8 = C.POINTER(C.c_uint8)
+P64 = C.POINTER(C.c_int64)
+VP = C.c_void_p
+
+# name -> (restype, argtypes); every exported symbol of include/cgc.h
+SIGNATURES = {
+    "cgc_last_error": (C.c_char_p, []),
+    "cgc_version": (C.c_char_p, []),
+    "cgc_init": (C.c_int, [C.c_int]),
+    "cgc_launch_count": (C.c_int64, []),
+    "cgc_grid_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, VP, C.POINTER(VP)]),
+    "cgc_grid_destroy": (C.c_int, [VP]),
+    "cgc_grid_set_tlinks": (C.c_int, [VP, VP, VP]),
+    "cgc_grid_set_nlinks": (C.c_int, [VP, C.c_int, VP, VP]),
+    "cgc_detect_grid": (C.c_int, [C.c_int32, C.c_int64, VP, VP, P32]),
+    "cgc_grid_create_from_edges": (C.c_int, [C.c_int32, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(VP), P32]),
+    "cgc_grid_set_tlinks_device": (C.c_int, [VP, VP, VP]),
+    "cgc_grid_set_nlinks_device": (C.c_int, [VP, C.c_int, VP, VP]),
+    "cgc_grid_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),
+    "cgc_grid_get_segments": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
+    "cgc_grid_get_segments_device": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
+    "cgc_grid_get_residuals": (C.c_int, [VP, C.POINTER(VP), VP, VP]),
+    "cgc_grid_stats": (C.c_int, [VP, C.POINTER(Stats)]),
+    "cgc_batch_create": (C.c_int, [C.c_int32, VP, VP, C.POINTER(VP)]),
+    "cgc_batch_destroy": (C.c_int, [VP]),
+    "cgc_batch_set_tlinks": (C.c_int, [VP, C.c_int32, VP, VP]),
+    "cgc_batch_set_nlinks": (C.c_int, [VP, C.c_int32, C.c_int, VP, VP]),
+    "cgc_batch_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),
+    "cgc_batch_get_segments": (C.c_int, [VP, C.c_int32, C.c_int, VP, C.c_uint8, C.c_uint8]),
+    "cgc_batch_stats": (C.c_int, [VP, C.POINTER(Stats)]),
+    "cgc_volume_preset": (C.c_int, [C.c_int, C.c_int32, C.POINTER(VolumeSpec)]),
+    "cgc_volume_generate": (C.c_int, [C.POINTER(VolumeSpec), VP, VP, VP, VP, VP, VP]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libcgc.so once; raises if it is absent (build it with
+    `python -m cugip_b200.build` or `__graft_entry__.build()`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libcgc.so not built: {path} is missing (run cugip_b200/build.py)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != CGC_OK:
+        raise CgcError(rc, load().cgc_last_error().decode(errors="replace"))
+
+
+def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
+            persistent: int = 0) -> Options:
+    o = Options()
+    o.struct_size = C.sizeof(Options)
+    o.local_pulses = local_pulses
+    o.sweeps_per_relabel = sweeps_per_relabel
+    o.schedule = schedule
+    o.max_sweeps = max_sweeps
+    o.persistent = persistent
+    return o

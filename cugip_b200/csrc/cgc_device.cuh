@@ -1,0 +1,79 @@
+// Device-side data structures and tile routines of the grid push-relabel engine.
+//
+// HBM layout.  Every instance is padded to whole 8x8x8 tiles; all instances of
+// a pool share one tile index space.  Each per-voxel quantity is a plane of
+// T*512 entries in tile-major ("blocked") order: voxel (x,y,z) of tile t sits
+// at t*512 + (x&7) + 8*(y&7) + 64*(z&7), so one tile of one plane is a
+// contiguous 2 KB run (fully coalesced, one 128-byte line per warp-row).
+//   e      int32  excess
+//   h      int32  height (distance label); INF = unreachable from the sink side
+//   rT     int32  residual of the sink t-link
+//   r[d]   int32  residual of the n-link to the neighbour in direction d
+//                 (d = +x,-x,+y,-y,+z,-z; 0 where the neighbour is outside)
+//   rmask  uint8  bit d: r[d] > 0, bit 6: rT > 0 (the BFS reads 1 byte, not 28)
+//   reach  uint8  source-side reachability (canonical cut)
+// Padding voxels have zero capacities everywhere and never become active.
+//
+// The residual graph of the reference is a CSR edge list with one residual
+// pair per undirected edge (include/cugip/advanced_operations/detail/edge_record.hpp:36-57,
+// graph_cut.hpp:239-290); on a grid the neighbours are implicit, so the
+// engine keeps one out-residual plane per direction instead.
+#pragma once
+#include <cstdint>
+
+namespace cgc {
+
+constexpr int TILE = 8;
+constexpr int TV = 512;            // voxels per tile
+constexpr int INF = 0x3fffffff;    // height of vertices that cannot reach the sink
+constexpr int HALO = 1000;         // 10x10x10 heights with a one-voxel halo
+
+enum Dir { PX = 0, MX = 1, PY = 2, MY = 3, PZ = 4, MZ = 5 };
+
+// counters in DevPool::cnt
+enum Counter {
+  C_BFS0 = 0,      // 3 BFS worklists
+  C_SW0 = 3,       // 4 sweep worklists
+  C_ACT = 7,       // active tiles after the last global relabel
+  C_ROUNDS = 8,    // BFS rounds executed
+  C_NCOUNTERS = 16
+};
+
+// statistics in DevPool::stats (unsigned long long)
+enum Stat { S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5, S_NSTATS = 8 };
+
+struct InstGeo {
+  int32_t X, Y, Z;      // voxel extents
+  int32_t TX, TY, TZ;   // tile extents
+  int32_t tile_base;    // first tile of the instance
+  int32_t hdead;        // heights >= hdead cannot reach the sink (voxel count)
+};
+
+struct DevPool {
+  int32_t T;            // tiles
+  int32_t ninst;
+  int64_t Np;           // T*512
+  int32_t* e;
+  int32_t* h;
+  int32_t* rT;
+  int32_t* r;           // 6 planes: r + d*Np
+  uint8_t* rmask;
+  uint8_t* reach;
+  const int32_t* nbr;   // 6*T: neighbour tile in direction d, -1 outside
+  const int32_t* tinst; // T: instance of the tile
+  const uint8_t* tpar;  // T: (tx+ty+tz)&1
+  uint8_t* act;         // T: tile holds an active voxel (e>0, h<INF)
+  uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
+  uint32_t* stamp_sw;   // T: last sweep the tile was queued for
+  int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
+  int32_t* cnt;         // C_NCOUNTERS
+  unsigned long long* flow;   // ninst: flow value (int64 as two's complement)
+  const InstGeo* geo;   // ninst
+  unsigned long long* stats;  // S_NSTATS
+  int32_t* err;         // first error code raised on the device
+  uint32_t* bar;        // grid barrier: [0] arrivals, [1] generation
+};
+
+__host__ __device__ inline int dir_axis(int d) { return d >> 1; }
+
+}  // namespace cgc

@@ -1,0 +1,840 @@
+// Kernels and host driver of the grid push-relabel engine, plus the C ABI.
+//
+// The host driver replaces MinCut::compute / MinimalGraphCutComputation::run
+// (include/cugip/advanced_operations/detail/graph_cut_implementation.hpp:122-198,
+// 286-308): preflow initialisation, then {exact global relabel; K sweep pairs}
+// until a global relabel finds no active voxel, then the cut sets.  With
+// `persistent` (the default) the whole loop runs inside one cooperative
+// launch whose phases are separated by a grid barrier with a bounded wait, so
+// no host round trip happens per BFS level or push level (the reference
+// synchronises and copies a counter back for every level,
+// detail/graph_cut_relabeling.hpp:962-984, detail/graph_cut_push.hpp:395-459).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cgc.h"
+#include "cgc_internal.h"
+#include "cgc_kernels.cuh"
+
+namespace cgc {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+static inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int ok() {
+  g_last_error.clear();
+  return CGC_OK;
+}
+
+#define CGC_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::cgc::fail(e_ == cudaErrorMemoryAllocation ? CGC_ERR_OOM : CGC_ERR_CUDA,      \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+// ===========================================================================
+// kernels
+// ===========================================================================
+
+// Copies the linear (x-fastest) t-link arrays of one instance into the
+// blocked e (= capS for now) and rT (= capT) planes.
+__global__ void __launch_bounds__(512) k_put_tlinks(DevPool P, int inst, const int32_t* __restrict__ capS,
+                                                    const int32_t* __restrict__ capT) {
+  const InstGeo G = P.geo[inst];
+  const int lt = blockIdx.x;
+  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
+  const int l = threadIdx.x;
+  const int x = tx * 8 + (l & 7), y = ty * 8 + ((l >> 3) & 7), z = tz * 8 + (l >> 6);
+  const int64_t g = (int64_t)(G.tile_base + lt) * TV + l;
+  int s = 0, c = 0;
+  if (x < G.X && y < G.Y && z < G.Z) {
+    const int64_t v = x + (int64_t)G.X * (y + (int64_t)G.Y * z);
+    s = capS[v]; c = capT[v];
+    if (s < 0 || c < 0) raise_error(P, CGC_ERR_ARG);
+  }
+  P.e[g] = s;
+  P.rT[g] = c;
+}
+
+// Copies the n-links of one axis: r[+a][v] = fwd[v], r[-a][v+e_a] = bwd[v].
+__global__ void __launch_bounds__(512) k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __restrict__ fwd,
+                                                    const int32_t* __restrict__ bwd) {
+  const InstGeo G = P.geo[inst];
+  const int lt = blockIdx.x;
+  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
+  const int l = threadIdx.x;
+  const int x = tx * 8 + (l & 7), y = ty * 8 + ((l >> 3) & 7), z = tz * 8 + (l >> 6);
+  const int64_t g = (int64_t)(G.tile_base + lt) * TV + l;
+  int f = 0, b = 0;
+  if (x < G.X && y < G.Y && z < G.Z) {
+    const int c = axis == 0 ? x : axis == 1 ? y : z;
+    const int ext = axis == 0 ? G.X : axis == 1 ? G.Y : G.Z;
+    const int64_t stride = axis == 0 ? 1 : axis == 1 ? (int64_t)G.X : (int64_t)G.X * G.Y;
+    const int64_t v = x + (int64_t)G.X * (y + (int64_t)G.Y * z);
+    if (fwd && c + 1 < ext) f = fwd[v];
+    if (bwd && c > 0) b = bwd[v - stride];
+    if (f < 0 || b < 0) raise_error(P, CGC_ERR_ARG);
+  }
+  P.r[(2 * axis) * P.Np + g] = f;
+  P.r[(2 * axis + 1) * P.Np + g] = b;
+}
+
+// Preflow initialisation (replaces initResidualsKernel and
+// pushThroughTLinksFromSourceKernel, graph_cut_implementation.hpp:28-40,
+// graph_cut_push.hpp:11-24): the t-links of a voxel cancel,
+// m = min(capS, capT) goes straight from the source to the sink, the rest of
+// capS becomes excess.  Also checks that no excess or residual can exceed
+// int32 and builds the residual bit mask.
+__global__ void __launch_bounds__(512) k_prepare(DevPool P) {
+  __shared__ long long red[16];
+  const int t = blockIdx.x;
+  const int l = threadIdx.x;
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  const int64_t g = (int64_t)t * TV + l;
+  const int64_t Np = P.Np;
+  const int s = P.e[g], c = P.rT[g];
+  const int mcap = min(s, c);
+  const int e = s - mcap, rT = c - mcap;
+  long long inflow = e;
+  unsigned m = rT > 0 ? 64u : 0u;
+  bool bad = false;
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    const int rv = P.r[d * Np + g];
+    int64_t ng;
+    bool has = true;
+    if (inside(d, x, y, z)) ng = (int64_t)t * TV + l + loff(d);
+    else {
+      const int nt = P.nbr[d * P.T + t];
+      has = nt >= 0;
+      ng = (int64_t)nt * TV + l + xoff(d);
+    }
+    const long long back = has ? (long long)P.r[(d ^ 1) * Np + ng] : 0ll;
+    if (!has && rv != 0) bad = true;  // capacity towards the outside of the grid
+    inflow += back;
+    if ((long long)rv + back > 2147483647ll) bad = true;
+    m |= (rv > 0 ? 1u : 0u) << d;
+  }
+  if (inflow > 2147483647ll) bad = true;
+  if (bad) raise_error(P, CGC_ERR_OVERFLOW);
+  P.e[g] = e;
+  P.rT[g] = rT;
+  P.h[g] = INF;
+  P.rmask[g] = (uint8_t)m;
+  P.reach[g] = 0;
+  const long long tot = block_sum64((long long)mcap, red);
+  if (l == 0) {
+    P.act[t] = 0;
+    if (tot) atomicAdd(P.flow + P.tinst[t], (unsigned long long)tot);
+  }
+}
+
+__global__ void k_zero_axis(DevPool P, int inst, int axis) {
+  const InstGeo G = P.geo[inst];
+  const int64_t n = (int64_t)G.TX * G.TY * G.TZ * TV;
+  const int64_t base = (int64_t)G.tile_base * TV;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    P.r[(2 * axis) * P.Np + base + i] = 0;
+    P.r[(2 * axis + 1) * P.Np + base + i] = 0;
+  }
+}
+
+// Host-driven schedule: one launch per sweep / BFS round.
+__global__ void __launch_bounds__(512, 2) k_sweep_list(DevPool P, const int32_t* list, const int32_t* cnt, int L) {
+  __shared__ SweepShared S;
+  const int n = *cnt;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) sweep_tile<false>(P, list[i], L, S, 0, nullptr, nullptr, 0, nullptr, nullptr);
+}
+
+__global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool pred = t < P.T && P.act[t] && P.tpar[t] == parity;
+  warp_append(pred, t, list, cnt);
+}
+
+__global__ void __launch_bounds__(512) k_bfs_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, id0, list0, cnt0);
+}
+
+__global__ void __launch_bounds__(512, 2) k_bfs_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
+                                                      int32_t* list_next, int32_t* cnt_next) {
+  __shared__ BfsShared S;
+  const int n = *cnt;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) bfs_tile(P, list[i], S, id_next, list_next, cnt_next);
+}
+
+__global__ void __launch_bounds__(512) k_reach_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  for (int t = blockIdx.x; t < P.T; t += gridDim.x) reach_init_tile(P, t, id0, list0, cnt0);
+}
+
+__global__ void __launch_bounds__(512, 2) k_reach_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
+                                                        int32_t* list_next, int32_t* cnt_next) {
+  __shared__ ReachShared S;
+  const int n = *cnt;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) reach_tile(P, list[i], S, id_next, list_next, cnt_next);
+}
+
+// ---------------------------------------------------------------------------
+// Grid-wide barrier for the cooperative (co-resident) launch.  Waits are
+// bounded: after `limit_ns` the waiting CTA records CGC_ERR_TIMEOUT and every
+// CTA leaves the kernel at its next barrier.
+__device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* gen = P.bar + 1;
+    const uint32_t g0 = *gen;
+    __threadfence();
+    const uint32_t arrived = atomicAdd(P.bar, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(P.bar, 0u);
+      __threadfence();
+      atomicAdd(P.bar + 1, 1u);
+    } else {
+      const uint64_t t0 = globaltimer_ns();
+      while (*gen == g0) {
+        __nanosleep(64);
+        if (globaltimer_ns() - t0 > limit_ns) { raise_error(P, CGC_ERR_TIMEOUT); break; }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int32_t*)P.err == 0;
+}
+
+__device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }
+
+struct SolveParams {
+  int L;                 // pulses per tile visit
+  int K;                 // sweep pairs between global relabels
+  int64_t max_sweeps;    // cap on sweeps (parity steps)
+  uint64_t limit_ns;     // bounded barrier wait
+};
+
+union SolveShared {
+  SweepShared sw;
+  BfsShared bfs;
+  ReachShared rc;
+};
+
+// The whole solve in one cooperative launch.
+__global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
+  int32_t* const sl[4] = {P.lists + 3 * P.T, P.lists + 4 * P.T, P.lists + 5 * P.T, P.lists + 6 * P.T};
+  int32_t* const bc = P.cnt + C_BFS0;
+  int32_t* const sc = P.cnt + C_SW0;
+  uint32_t bfs_id = 1;
+  int64_t s = 0;        // sweep index; sweep s uses list s&3 and stamp id s+1
+  int64_t sweeps = 0;
+  long long rounds = 0, relabels = 0;
+  for (;;) {
+    // ------------------------------------------------ exact global relabel
+    if (b == 0 && tid == 0) {
+      bc[0] = bc[1] = bc[2] = 0;
+      sc[0] = sc[1] = sc[2] = sc[3] = 0;
+    }
+    if (!grid_sync(P, prm.limit_ns)) return;
+    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, bfs_id, bl[0], bc + 0);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    int k = 0;
+    for (;;) {
+      const int n = ld_cnt(bc + k % 3);
+      if (n == 0) break;
+      if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
+      for (int i = b; i < n; i += G) bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+      ++k;
+      if (!grid_sync(P, prm.limit_ns)) return;
+    }
+    bfs_id += k + 1;
+    rounds += k;
+    ++relabels;
+    // ------------------------------------------------ active tiles -> parity lists
+    s += 2;  // fresh stamp ids for the lists built here
+    for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
+      if (__ldcg(P.act + t)) {
+        const int par = __ldcg(P.tpar + t);
+        P.stamp_sw[t] = (uint32_t)(s + par + 1);
+        sl[(s + par) & 3][atomicAdd(sc + ((s + par) & 3), 1)] = t;
+      }
+    }
+    if (!grid_sync(P, prm.limit_ns)) return;
+    const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));
+    if (nact == 0) break;
+    if (sweeps >= prm.max_sweeps) {
+      if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
+      break;
+    }
+    // ------------------------------------------------ sweeps
+    for (int j = 0; j < 2 * prm.K; ++j, ++s) {
+      const int n = ld_cnt(sc + (s & 3));
+      if (n == 0 && ld_cnt(sc + ((s + 1) & 3)) == 0) break;
+      if (b == 0 && tid == 0) sc[(s + 3) & 3] = 0;
+      for (int i = b; i < n; i += G)
+        sweep_tile<true>(P, __ldcg(sl[s & 3] + i), prm.L, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3));
+      ++sweeps;
+      if (!grid_sync(P, prm.limit_ns)) return;
+    }
+  }
+  // ------------------------------------------------ source-side reachability
+  if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
+  if (!grid_sync(P, prm.limit_ns)) return;
+  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, bfs_id, bl[0], bc + 0);
+  if (!grid_sync(P, prm.limit_ns)) return;
+  int k = 0;
+  for (;;) {
+    const int n = ld_cnt(bc + k % 3);
+    if (n == 0) break;
+    if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
+    for (int i = b; i < n; i += G) reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+    ++k;
+    if (!grid_sync(P, prm.limit_ns)) return;
+  }
+  if (b == 0 && tid == 0) {
+    P.stats[S_SWEEPS] = (unsigned long long)sweeps;
+    P.stats[S_RELABELS] = (unsigned long long)relabels;
+    P.stats[S_ROUNDS] = (unsigned long long)rounds;
+  }
+}
+
+// Output kernels (linear layout of one instance).
+__global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg) {
+  const InstGeo G = P.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(v % G.X), y = (int)((v / G.X) % G.Y), z = (int)(v / ((int64_t)G.X * G.Y));
+    const int64_t t = G.tile_base + (x >> 3) + G.TX * ((y >> 3) + G.TY * (z >> 3));
+    const int64_t g = t * TV + (x & 7) + 8 * (y & 7) + 64 * (z & 7);
+    const bool in = which == CGC_SEG_SINK_REACH ? (P.h[g] < INF) : (P.reach[g] != 0);
+    out[v] = in ? mask : bg;
+  }
+}
+
+__global__ void k_unpermute(DevPool P, int inst, const int32_t* plane, int32_t* out) {
+  const InstGeo G = P.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(v % G.X), y = (int)((v / G.X) % G.Y), z = (int)(v / ((int64_t)G.X * G.Y));
+    const int64_t t = G.tile_base + (x >> 3) + G.TX * ((y >> 3) + G.TY * (z >> 3));
+    out[v] = plane[t * TV + (x & 7) + 8 * (y & 7) + 64 * (z & 7)];
+  }
+}
+
+// ===========================================================================
+// host side
+// ===========================================================================
+
+struct Pool {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int ninst = 0;
+  std::vector<InstGeo> geo;
+  std::vector<uint32_t> uploaded;  // bit 0 tlinks, bits 1..3 axes
+  int64_t maxN = 0;
+  int32_t T = 0;
+  int64_t Np = 0;
+  DevPool dp{};
+  void* dbuf = nullptr;          // all device state
+  int32_t* staging = nullptr;    // 2*maxN int32
+  uint8_t* seg = nullptr;        // maxN bytes
+  int32_t* pinned_cnt = nullptr; // host-pinned counters
+  bool solved = false;
+  int sms = 148;
+  int coop_blocks = 0;           // co-resident CTAs of k_solve
+  int sweep_blocks = 0;
+  cgc_stats st{};
+  std::vector<int64_t> flows;
+  ~Pool() {
+    if (dbuf) cudaFree(dbuf);
+    if (staging) cudaFree(staging);
+    if (seg) cudaFree(seg);
+    if (pinned_cnt) cudaFreeHost(pinned_cnt);
+  }
+};
+
+static int check_device_error(Pool& p, const char* where) {
+  int32_t err = 0;
+  CGC_CUDA(cudaMemcpyAsync(&err, p.dp.err, sizeof(int32_t), cudaMemcpyDeviceToHost, p.stream));
+  CGC_CUDA(cudaStreamSynchronize(p.stream));
+  if (err == 0) return CGC_OK;
+  const char* what = err == CGC_ERR_OVERFLOW ? "capacities may overflow int32 excess/residuals (or a capacity points outside the grid)"
+                   : err == CGC_ERR_ARG ? "negative capacity"
+                   : err == CGC_ERR_TIMEOUT ? "a device-side wait timed out"
+                   : err == CGC_ERR_NOT_CONVERGED ? "max_sweeps reached before convergence"
+                   : "device error";
+  return fail(err, std::string(where) + ": " + what);
+}
+
+static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
+  if (!out || count <= 0 || !ext) return fail(CGC_ERR_ARG, "create: bad arguments");
+  std::unique_ptr<Pool> p(new (std::nothrow) Pool());
+  if (!p) return fail(CGC_ERR_OOM, "create: host allocation");
+  CGC_CUDA(cudaGetDevice(&p->device));
+  p->stream = (cudaStream_t)stream;
+  p->ninst = count;
+  int64_t T = 0;
+  for (int i = 0; i < count; ++i) {
+    const int32_t X = ext[3 * i], Y = ext[3 * i + 1], Z = ext[3 * i + 2];
+    if (X <= 0 || Y <= 0 || Z <= 0) return fail(CGC_ERR_ARG, "create: extents must be positive");
+    InstGeo G{};
+    G.X = X; G.Y = Y; G.Z = Z;
+    G.TX = (X + 7) / 8; G.TY = (Y + 7) / 8; G.TZ = (Z + 7) / 8;
+    G.tile_base = (int32_t)T;
+    const int64_t n = (int64_t)X * Y * Z;
+    if (n >= (int64_t)INF) return fail(CGC_ERR_ARG, "create: instance too large for int32 heights");
+    G.hdead = (int32_t)n;
+    T += (int64_t)G.TX * G.TY * G.TZ;
+    if (T > (int64_t)1 << 30) return fail(CGC_ERR_ARG, "create: too many tiles");
+    p->maxN = std::max(p->maxN, n);
+    p->geo.push_back(G);
+  }
+  p->T = (int32_t)T;
+  p->Np = T * TV;
+  p->uploaded.assign(count, 0u);
+  p->flows.assign(count, 0);
+
+  // one device allocation for all state (planes first, 256-byte aligned pieces)
+  const int64_t Np = p->Np;
+  auto al = [](int64_t b) { return (b + 255) & ~(int64_t)255; };
+  int64_t off = 0;
+  const int64_t o_e = off; off += al(Np * 4);
+  const int64_t o_h = off; off += al(Np * 4);
+  const int64_t o_rT = off; off += al(Np * 4);
+  const int64_t o_r = off; off += al(6 * Np * 4);
+  const int64_t o_rm = off; off += al(Np);
+  const int64_t o_rc = off; off += al(Np);
+  const int64_t o_nbr = off; off += al(6 * T * 4);
+  const int64_t o_ti = off; off += al(T * 4);
+  const int64_t o_tp = off; off += al(T);
+  const int64_t o_act = off; off += al(T);
+  const int64_t o_sb = off; off += al(T * 4);
+  const int64_t o_ss = off; off += al(T * 4);
+  const int64_t o_li = off; off += al(7 * T * 4);
+  const int64_t o_cnt = off; off += al(C_NCOUNTERS * 4);
+  const int64_t o_fl = off; off += al((int64_t)count * 8);
+  const int64_t o_geo = off; off += al((int64_t)count * sizeof(InstGeo));
+  const int64_t o_st = off; off += al(S_NSTATS * 8);
+  const int64_t o_err = off; off += al(4);
+  const int64_t o_bar = off; off += al(8);
+  CGC_CUDA(cudaMalloc(&p->dbuf, off));
+  CGC_CUDA(cudaMemsetAsync(p->dbuf, 0, off, p->stream));
+  char* base = (char*)p->dbuf;
+  DevPool& d = p->dp;
+  d.T = p->T; d.ninst = count; d.Np = Np;
+  d.e = (int32_t*)(base + o_e); d.h = (int32_t*)(base + o_h); d.rT = (int32_t*)(base + o_rT);
+  d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
+  d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
+  d.act = (uint8_t*)(base + o_act); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
+  d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
+  d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
+  d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
+
+  // tile tables
+  std::vector<int32_t> nbr(6 * (size_t)T, -1), ti((size_t)T);
+  std::vector<uint8_t> tp((size_t)T);
+  for (int i = 0; i < count; ++i) {
+    const InstGeo& G = p->geo[i];
+    for (int tz = 0; tz < G.TZ; ++tz)
+      for (int ty = 0; ty < G.TY; ++ty)
+        for (int tx = 0; tx < G.TX; ++tx) {
+          const int64_t t = G.tile_base + tx + (int64_t)G.TX * (ty + (int64_t)G.TY * tz);
+          ti[t] = i;
+          tp[t] = (uint8_t)((tx + ty + tz) & 1);
+          auto id = [&](int a, int b2, int c) -> int32_t {
+            if (a < 0 || b2 < 0 || c < 0 || a >= G.TX || b2 >= G.TY || c >= G.TZ) return -1;
+            return (int32_t)(G.tile_base + a + (int64_t)G.TX * (b2 + (int64_t)G.TY * c));
+          };
+          nbr[PX * T + t] = id(tx + 1, ty, tz); nbr[MX * T + t] = id(tx - 1, ty, tz);
+          nbr[PY * T + t] = id(tx, ty + 1, tz); nbr[MY * T + t] = id(tx, ty - 1, tz);
+          nbr[PZ * T + t] = id(tx, ty, tz + 1); nbr[MZ * T + t] = id(tx, ty, tz - 1);
+        }
+  }
+  CGC_CUDA(cudaMemcpyAsync((void*)d.nbr, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, p->stream));
+  CGC_CUDA(cudaMemcpyAsync((void*)d.tinst, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, p->stream));
+  CGC_CUDA(cudaMemcpyAsync((void*)d.tpar, tp.data(), tp.size(), cudaMemcpyHostToDevice, p->stream));
+  CGC_CUDA(cudaMemcpyAsync((void*)d.geo, p->geo.data(), p->geo.size() * sizeof(InstGeo), cudaMemcpyHostToDevice, p->stream));
+  CGC_CUDA(cudaMalloc(&p->staging, 2 * p->maxN * 4));
+  CGC_CUDA(cudaMalloc(&p->seg, p->maxN));
+  CGC_CUDA(cudaMallocHost(&p->pinned_cnt, 64 * 4));
+
+  cudaDeviceProp prop;
+  CGC_CUDA(cudaGetDeviceProperties(&prop, p->device));
+  p->sms = prop.multiProcessorCount;
+  int occ = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, 512, 0));
+  p->coop_blocks = std::max(1, occ) * p->sms;
+  int occ2 = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_sweep_list, 512, 0));
+  p->sweep_blocks = std::max(1, occ2) * p->sms;
+  CGC_CUDA(cudaStreamSynchronize(p->stream));
+  *out = p.release();
+  return ok();
+}
+
+static int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host) {
+  if (inst < 0 || inst >= p.ninst || !capS || !capT) return fail(CGC_ERR_ARG, "set_tlinks: bad arguments");
+  const InstGeo& G = p.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  const int32_t *s = capS, *c = capT;
+  if (host) {
+    CGC_CUDA(cudaMemcpyAsync(p.staging, capS, N * 4, cudaMemcpyHostToDevice, p.stream));
+    CGC_CUDA(cudaMemcpyAsync(p.staging + p.maxN, capT, N * 4, cudaMemcpyHostToDevice, p.stream));
+    s = p.staging; c = p.staging + p.maxN;
+  }
+  k_put_tlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, s, c); note_launch();
+  CGC_CUDA(cudaGetLastError());
+  p.uploaded[inst] |= 1u;
+  p.solved = false;
+  return ok();
+}
+
+static int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host) {
+  if (inst < 0 || inst >= p.ninst || axis < 0 || axis > 2 || !fwd || !bwd)
+    return fail(CGC_ERR_ARG, "set_nlinks: bad arguments");
+  const InstGeo& G = p.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  const int32_t *f = fwd, *b = bwd;
+  if (host) {
+    CGC_CUDA(cudaMemcpyAsync(p.staging, fwd, N * 4, cudaMemcpyHostToDevice, p.stream));
+    f = p.staging;
+    if (bwd == fwd) b = p.staging;
+    else {
+      CGC_CUDA(cudaMemcpyAsync(p.staging + p.maxN, bwd, N * 4, cudaMemcpyHostToDevice, p.stream));
+      b = p.staging + p.maxN;
+    }
+  }
+  k_put_nlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, axis, f, b); note_launch();
+  CGC_CUDA(cudaGetLastError());
+  p.uploaded[inst] |= 2u << axis;
+  p.solved = false;
+  return ok();
+}
+
+static cgc_options resolve_options(const cgc_options* o) {
+  cgc_options r{};
+  r.struct_size = sizeof(cgc_options);
+  r.local_pulses = 16;
+  r.sweeps_per_relabel = 8;
+  r.schedule = CGC_SCHED_PARITY;
+  r.max_sweeps = 1 << 20;
+  r.persistent = 1;
+  if (o) {
+    if (o->local_pulses > 0) r.local_pulses = std::min(o->local_pulses, 64);
+    if (o->sweeps_per_relabel > 0) r.sweeps_per_relabel = o->sweeps_per_relabel;
+    if (o->schedule) r.schedule = o->schedule;
+    if (o->max_sweeps > 0) r.max_sweeps = o->max_sweeps;
+    if (o->persistent) r.persistent = o->persistent;
+  }
+  return r;
+}
+
+// host-driven BFS (or reachability) pass; returns rounds executed
+template <bool REACH>
+static int host_bfs(Pool& p, uint32_t& id, int64_t& rounds) {
+  DevPool& d = p.dp;
+  int32_t* bl[3] = {d.lists, d.lists + d.T, d.lists + 2 * d.T};
+  CGC_CUDA(cudaMemsetAsync(d.cnt + C_BFS0, 0, 3 * 4, p.stream));
+  const int gi = std::min<int>(d.T, p.sms * 8);
+  if (REACH) { k_reach_init<<<gi, 512, 0, p.stream>>>(d, id, bl[0], d.cnt + C_BFS0); note_launch(); }
+  else { k_bfs_init<<<gi, 512, 0, p.stream>>>(d, id, bl[0], d.cnt + C_BFS0); note_launch(); }
+  CGC_CUDA(cudaGetLastError());
+  for (int k = 0;; ++k) {
+    CGC_CUDA(cudaMemcpyAsync(p.pinned_cnt, d.cnt + C_BFS0 + k % 3, 4, cudaMemcpyDeviceToHost, p.stream));
+    CGC_CUDA(cudaStreamSynchronize(p.stream));
+    const int n = p.pinned_cnt[0];
+    if (n == 0) { id += k + 1; break; }
+    CGC_CUDA(cudaMemsetAsync(d.cnt + C_BFS0 + (k + 1) % 3, 0, 4, p.stream));
+    const int gb = std::min(n, p.sweep_blocks);
+    if (REACH) { k_reach_round<<<gb, 512, 0, p.stream>>>(d, bl[k % 3], d.cnt + C_BFS0 + k % 3, id + k + 1, bl[(k + 1) % 3], d.cnt + C_BFS0 + (k + 1) % 3); note_launch(); }
+    else { k_bfs_round<<<gb, 512, 0, p.stream>>>(d, bl[k % 3], d.cnt + C_BFS0 + k % 3, id + k + 1, bl[(k + 1) % 3], d.cnt + C_BFS0 + (k + 1) % 3); note_launch(); }
+    CGC_CUDA(cudaGetLastError());
+    ++rounds;
+  }
+  return CGC_OK;
+}
+
+static int pool_solve(Pool& p, const cgc_options* opts) {
+  const cgc_options o = resolve_options(opts);
+  DevPool& d = p.dp;
+  for (int i = 0; i < p.ninst; ++i) {
+    if (!(p.uploaded[i] & 1u)) return fail(CGC_ERR_STATE, "maxflow: set_tlinks was not called since the last solve");
+    for (int a = 0; a < 3; ++a)
+      if (!(p.uploaded[i] & (2u << a))) {
+        const InstGeo& G = p.geo[i];
+        k_zero_axis<<<std::max(1, std::min(G.TX * G.TY * G.TZ, 1024)), 512, 0, p.stream>>>(d, i, a); note_launch();
+      }
+  }
+  const long long launches0 = g_launches.load();
+  cudaEvent_t ev0, ev1, evk0, evk1;
+  CGC_CUDA(cudaEventCreate(&ev0));
+  CGC_CUDA(cudaEventCreate(&ev1));
+  CGC_CUDA(cudaEventCreate(&evk0));
+  CGC_CUDA(cudaEventCreate(&evk1));
+  CGC_CUDA(cudaEventRecord(ev0, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.flow, 0, (size_t)p.ninst * 8, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.stats, 0, S_NSTATS * 8, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.err, 0, 4, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, p.stream));
+  k_prepare<<<d.T, 512, 0, p.stream>>>(d); note_launch();
+  CGC_CUDA(cudaGetLastError());
+  int rc = check_device_error(p, "maxflow");
+  auto destroy_events = [&]() { cudaEventDestroy(ev0); cudaEventDestroy(ev1); cudaEventDestroy(evk0); cudaEventDestroy(evk1); };
+  if (rc) { destroy_events(); return rc; }
+
+  int64_t sweeps = 0, relabels = 0, rounds = 0;
+  if (o.persistent > 0) {
+    SolveParams prm;
+    prm.L = o.local_pulses;
+    prm.K = o.sweeps_per_relabel;
+    prm.max_sweeps = (int64_t)o.max_sweeps;
+    prm.limit_ns = 20ull * 1000000000ull;
+    void* args[] = {(void*)&d, (void*)&prm};
+    CGC_CUDA(cudaEventRecord(evk0, p.stream));
+    CGC_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve, dim3(p.coop_blocks), dim3(512), args, 0, p.stream));
+    note_launch();
+    CGC_CUDA(cudaEventRecord(evk1, p.stream));
+  } else {
+    CGC_CUDA(cudaEventRecord(evk0, p.stream));
+    uint32_t id = 1;
+    int32_t* sl = d.lists + 3 * d.T;
+    for (;;) {
+      rc = host_bfs<false>(p, id, rounds);
+      if (rc) break;
+      ++relabels;
+      CGC_CUDA(cudaMemsetAsync(d.cnt + C_SW0, 0, 8, p.stream));
+      k_compact<<<(d.T + 255) / 256, 256, 0, p.stream>>>(d, 0, sl, d.cnt + C_SW0); note_launch();
+      k_compact<<<(d.T + 255) / 256, 256, 0, p.stream>>>(d, 1, sl + d.T, d.cnt + C_SW0 + 1); note_launch();
+      CGC_CUDA(cudaMemcpyAsync(p.pinned_cnt, d.cnt + C_SW0, 8, cudaMemcpyDeviceToHost, p.stream));
+      CGC_CUDA(cudaStreamSynchronize(p.stream));
+      if (p.pinned_cnt[0] + p.pinned_cnt[1] == 0) break;
+      if (sweeps >= o.max_sweeps) { rc = fail(CGC_ERR_NOT_CONVERGED, "maxflow: max_sweeps reached"); break; }
+      for (int j = 0; j < 2 * o.sweeps_per_relabel; ++j) {
+        const int par = j & 1;
+        if (j > 0) {
+          CGC_CUDA(cudaMemsetAsync(d.cnt + C_SW0 + par, 0, 4, p.stream));
+          k_compact<<<(d.T + 255) / 256, 256, 0, p.stream>>>(d, par, sl + par * d.T, d.cnt + C_SW0 + par); note_launch();
+        }
+        k_sweep_list<<<p.sweep_blocks, 512, 0, p.stream>>>(d, sl + par * d.T, d.cnt + C_SW0 + par, o.local_pulses); note_launch();
+        CGC_CUDA(cudaGetLastError());
+        ++sweeps;
+      }
+    }
+    if (!rc) rc = host_bfs<true>(p, id, rounds);
+    CGC_CUDA(cudaEventRecord(evk1, p.stream));
+  }
+  CGC_CUDA(cudaEventRecord(ev1, p.stream));
+  if (!rc) rc = check_device_error(p, "maxflow");
+  float ms = 0.f, kms = 0.f;
+  if (!rc) {
+    CGC_CUDA(cudaEventSynchronize(ev1));
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventElapsedTime(&kms, evk0, evk1);
+  }
+  destroy_events();
+  if (rc) return rc;
+
+  unsigned long long stats[S_NSTATS];
+  CGC_CUDA(cudaMemcpy(stats, d.stats, sizeof(stats), cudaMemcpyDeviceToHost));
+  CGC_CUDA(cudaMemcpy(p.flows.data(), d.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToHost));
+  std::memset(&p.st, 0, sizeof(p.st));
+  p.st.flow = 0;
+  for (int64_t f : p.flows) p.st.flow += f;
+  if (o.persistent > 0) {
+    p.st.sweeps = (int64_t)stats[S_SWEEPS];
+    p.st.global_relabels = (int64_t)stats[S_RELABELS];
+    p.st.bfs_rounds = (int64_t)stats[S_ROUNDS];
+  } else {
+    p.st.sweeps = sweeps;
+    p.st.global_relabels = relabels;
+    p.st.bfs_rounds = rounds;
+  }
+  p.st.tiles_swept = (int64_t)stats[S_TILES_SWEPT];
+  p.st.tiles_relabelled = (int64_t)stats[S_TILES_BFS];
+  p.st.pulses = (int64_t)stats[S_PULSES];
+  p.st.solve_ms = ms;
+  p.st.kernel_ms = kms;
+  p.st.launches = g_launches.load() - launches0;
+  for (auto& u : p.uploaded) u = 0;
+  p.solved = true;
+  return ok();
+}
+
+static int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host) {
+  if (inst < 0 || inst >= p.ninst || !out || (which != CGC_SEG_SINK_REACH && which != CGC_SEG_SOURCE_MIN))
+    return fail(CGC_ERR_ARG, "get_segments: bad arguments");
+  if (!p.solved) return fail(CGC_ERR_STATE, "get_segments: call maxflow first");
+  const InstGeo& G = p.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  uint8_t* dst = host ? p.seg : out;
+  const int blocks = (int)std::min<int64_t>((N + 255) / 256, 65535);
+  k_segments<<<blocks, 256, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
+  CGC_CUDA(cudaGetLastError());
+  if (host) CGC_CUDA(cudaMemcpyAsync(out, p.seg, N, cudaMemcpyDeviceToHost, p.stream));
+  CGC_CUDA(cudaStreamSynchronize(p.stream));
+  return ok();
+}
+
+static int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess) {
+  if (inst < 0 || inst >= p.ninst) return fail(CGC_ERR_ARG, "get_residuals: bad instance");
+  if (!p.solved) return fail(CGC_ERR_STATE, "get_residuals: call maxflow first");
+  const InstGeo& G = p.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  const int blocks = (int)std::min<int64_t>((N + 255) / 256, 65535);
+  auto one = [&](const int32_t* plane, int32_t* out) -> int {
+    if (!out) return CGC_OK;
+    k_unpermute<<<blocks, 256, 0, p.stream>>>(p.dp, inst, plane, p.staging); note_launch();
+    CGC_CUDA(cudaGetLastError());
+    CGC_CUDA(cudaMemcpyAsync(out, p.staging, N * 4, cudaMemcpyDeviceToHost, p.stream));
+    CGC_CUDA(cudaStreamSynchronize(p.stream));
+    return CGC_OK;
+  };
+  int rc;
+  if (res)
+    for (int d = 0; d < 6; ++d)
+      if ((rc = one(p.dp.r + d * p.Np, res[d]))) return rc;
+  if ((rc = one(p.dp.rT, resT))) return rc;
+  if ((rc = one(p.dp.e, excess))) return rc;
+  return ok();
+}
+
+}  // namespace cgc
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using cgc::Pool;
+
+struct cgc_grid { Pool* p; };
+struct cgc_batch { Pool* p; };
+
+extern "C" {
+
+const char* cgc_last_error(void) { return cgc::g_last_error.c_str(); }
+const char* cgc_version(void) { return "cgc 0.1 (sm_100a)"; }
+int64_t cgc_launch_count(void) { return (int64_t)cgc::g_launches.load(); }
+
+int cgc_init(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return cgc::fail(CGC_ERR_NO_DEVICE, "cgc_init: no CUDA device");
+  if (device < 0 || device >= n) return cgc::fail(CGC_ERR_ARG, "cgc_init: bad device index");
+  CGC_CUDA(cudaSetDevice(device));
+  CGC_CUDA(cudaFree(nullptr));
+  return cgc::ok();
+}
+
+int cgc_grid_create(int32_t X, int32_t Y, int32_t Z, void* stream, cgc_grid** out) {
+  if (!out) return cgc::fail(CGC_ERR_ARG, "cgc_grid_create: null output");
+  int32_t ext[3] = {X, Y, Z};
+  Pool* p = nullptr;
+  int rc = cgc::pool_create(1, ext, stream, &p);
+  if (rc) return rc;
+  *out = new cgc_grid{p};
+  return cgc::ok();
+}
+int cgc_grid_destroy(cgc_grid* g) {
+  if (!g) return cgc::ok();
+  delete g->p;
+  delete g;
+  return cgc::ok();
+}
+int cgc_grid_set_tlinks(cgc_grid* g, const int32_t* capS, const int32_t* capT) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_put_tlinks(*g->p, 0, capS, capT, true);
+}
+int cgc_grid_set_nlinks(cgc_grid* g, int axis, const int32_t* fwd, const int32_t* bwd) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_put_nlinks(*g->p, 0, axis, fwd, bwd, true);
+}
+int cgc_grid_set_tlinks_device(cgc_grid* g, const int32_t* capS, const int32_t* capT) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_put_tlinks(*g->p, 0, capS, capT, false);
+}
+int cgc_grid_set_nlinks_device(cgc_grid* g, int axis, const int32_t* fwd, const int32_t* bwd) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_put_nlinks(*g->p, 0, axis, fwd, bwd, false);
+}
+int cgc_grid_maxflow(cgc_grid* g, const cgc_options* opts, int64_t* flow) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  int rc = cgc::pool_solve(*g->p, opts);
+  if (rc) return rc;
+  if (flow) *flow = g->p->flows[0];
+  return cgc::ok();
+}
+int cgc_grid_get_segments(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_segments(*g->p, 0, which, out, mask, background, true);
+}
+int cgc_grid_get_segments_device(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_segments(*g->p, 0, which, out, mask, background, false);
+}
+int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, int32_t* excess) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_residuals(*g->p, 0, res, resT, excess);
+}
+int cgc_grid_stats(cgc_grid* g, cgc_stats* out) {
+  if (!g || !out) return cgc::fail(CGC_ERR_ARG, "null argument");
+  *out = g->p->st;
+  return cgc::ok();
+}
+
+int cgc_batch_create(int32_t count, const int32_t* extents, void* stream, cgc_batch** out) {
+  if (!out) return cgc::fail(CGC_ERR_ARG, "cgc_batch_create: null output");
+  Pool* p = nullptr;
+  int rc = cgc::pool_create(count, extents, stream, &p);
+  if (rc) return rc;
+  *out = new cgc_batch{p};
+  return cgc::ok();
+}
+int cgc_batch_destroy(cgc_batch* b) {
+  if (!b) return cgc::ok();
+  delete b->p;
+  delete b;
+  return cgc::ok();
+}
+int cgc_batch_set_tlinks(cgc_batch* b, int32_t i, const int32_t* capS, const int32_t* capT) {
+  if (!b) return cgc::fail(CGC_ERR_ARG, "null batch");
+  return cgc::pool_put_tlinks(*b->p, i, capS, capT, true);
+}
+int cgc_batch_set_nlinks(cgc_batch* b, int32_t i, int axis, const int32_t* fwd, const int32_t* bwd) {
+  if (!b) return cgc::fail(CGC_ERR_ARG, "null batch");
+  return cgc::pool_put_nlinks(*b->p, i, axis, fwd, bwd, true);
+}
+int cgc_batch_maxflow(cgc_batch* b, const cgc_options* opts, int64_t* flows) {
+  if (!b) return cgc::fail(CGC_ERR_ARG, "null batch");
+  int rc = cgc::pool_solve(*b->p, opts);
+  if (rc) return rc;
+  if (flows) std::memcpy(flows, b->p->flows.data(), b->p->flows.size() * 8);
+  return cgc::ok();
+}
+int cgc_batch_get_segments(cgc_batch* b, int32_t i, int which, uint8_t* out, uint8_t mask, uint8_t background) {
+  if (!b) return cgc::fail(CGC_ERR_ARG, "null batch");
+  return cgc::pool_segments(*b->p, i, which, out, mask, background, true);
+}
+int cgc_batch_stats(cgc_batch* b, cgc_stats* out) {
+  if (!b || !out) return cgc::fail(CGC_ERR_ARG, "null argument");
+  *out = b->p->st;
+  return cgc::ok();
+}
+
+}  // extern "C"

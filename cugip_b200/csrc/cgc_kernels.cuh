@@ -1,0 +1,384 @@
+// Tile routines and kernels of the grid push-relabel engine (sm_100a).
+//
+// One CTA of 512 threads owns one 8x8x8 tile at a time; thread l owns voxel
+// (l&7, (l>>3)&7, l>>6).  The voxel's own state (excess, height, sink
+// residual, six out-residuals) lives in registers; heights of the tile plus a
+// one-voxel halo live in shared memory so that neighbours can be read.
+//
+// Push sweep (replaces the per-level push of
+// include/cugip/advanced_operations/detail/graph_cut_push.hpp:160-186,236-318,
+// 461-482).  A visit runs up to L synchronous pulses of the Goldberg-Tarjan
+// parallel push-relabel inside the tile: every active voxel (e>0, h<INF)
+// pushes to the sink if h==1 and along every admissible residual edge
+// (h(u)==h(v)-1), then every voxel that is still active and has no
+// admissible edge relabels to 1+min over its residual neighbours.  Labels are
+// fixed during a push step and relabels read the old labels, so the labelling
+// stays valid.  Under the parity schedule only tiles with (tx+ty+tz) of one
+// parity run at a time; face neighbours always have the other parity, so the
+// halo heights are exact and the tile's pushes across a face (int32 atomics on
+// the neighbour's excess, plain adds on the neighbour's reverse residual,
+// which has a single writer) are ordinary valid pushes.
+//
+// Global relabel (replaces the level-synchronous BFS of
+// detail/graph_cut_relabeling.hpp:47-112,651-751,1004-1029).  Exact BFS
+// distance to the sink over reverse residual edges, computed by tile-local
+// Bellman-Ford relaxation to a fixed point in shared memory; a tile whose face
+// heights dropped re-queues its face neighbours.  Vertices the BFS does not
+// reach keep INF, which is the gap heuristic.
+//
+// Exact sink flow.  Pushes to the sink are capped by the sink residual (the
+// reference moves all excess of any sink-adjacent vertex,
+// detail/graph_cut_push.hpp:26-41); the flow is accumulated in int64.
+#pragma once
+#include <cuda_runtime.h>
+#include "cgc.h"
+#include "cgc_device.cuh"
+
+namespace cgc {
+
+__device__ __forceinline__ int halo_index(int x, int y, int z) { return (z + 1) * 100 + (y + 1) * 10 + (x + 1); }
+
+// offsets of the 6 neighbours in the halo array and inside a tile
+__device__ __forceinline__ int hoff(int d) {
+  return d == PX ? 1 : d == MX ? -1 : d == PY ? 10 : d == MY ? -10 : d == PZ ? 100 : -100;
+}
+__device__ __forceinline__ int loff(int d) {
+  return d == PX ? 1 : d == MX ? -1 : d == PY ? 8 : d == MY ? -8 : d == PZ ? 64 : -64;
+}
+// local index in the neighbouring tile when stepping out of the tile along d
+__device__ __forceinline__ int xoff(int d) {
+  return d == PX ? -7 : d == MX ? 7 : d == PY ? -56 : d == MY ? 56 : d == PZ ? -448 : 448;
+}
+__device__ __forceinline__ bool inside(int d, int x, int y, int z) {
+  return d == PX ? x < 7 : d == MX ? x > 0 : d == PY ? y < 7 : d == MY ? y > 0 : d == PZ ? z < 7 : z > 0;
+}
+// bit mask of the faces of the tile the voxel lies on
+__device__ __forceinline__ int face_bits(int x, int y, int z) {
+  return ((x == 7) << PX) | ((x == 0) << MX) | ((y == 7) << PY) | ((y == 0) << MY) | ((z == 7) << PZ) | ((z == 0) << MZ);
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void raise_error(const DevPool& P, int code) { atomicCAS(P.err, 0, code); }
+
+// Face f of the halo: thread k in [0,64) of face f writes halo entry (a,b) of
+// that face from the neighbouring tile (INF outside the grid).
+template <typename F>
+__device__ __forceinline__ void for_halo_entry(int l, F&& fn) {
+  if (l < 384) {
+    const int f = l >> 6, k = l & 63, a = k & 7, b = k >> 3;
+    int hi, src;
+    switch (f) {
+      case PX: hi = (b + 1) * 100 + (a + 1) * 10 + 9; src = 8 * a + 64 * b; break;
+      case MX: hi = (b + 1) * 100 + (a + 1) * 10;     src = 7 + 8 * a + 64 * b; break;
+      case PY: hi = (b + 1) * 100 + 90 + (a + 1);     src = a + 64 * b; break;
+      case MY: hi = (b + 1) * 100 + (a + 1);          src = a + 56 + 64 * b; break;
+      case PZ: hi = 900 + (b + 1) * 10 + (a + 1);     src = a + 8 * b; break;
+      default: hi = (b + 1) * 10 + (a + 1);           src = a + 8 * b + 448; break;
+    }
+    fn(f, hi, src);
+  }
+}
+
+__device__ __forceinline__ void load_halo_heights(const DevPool& P, int t, int* sh) {
+  for_halo_entry(threadIdx.x, [&](int f, int hi, int src) {
+    const int nt = __ldcg(P.nbr + f * P.T + t);
+    sh[hi] = (nt >= 0) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
+  });
+}
+
+// warp-aggregated append of `pred` items to list/cnt
+__device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t* list, int32_t* cnt) {
+  const unsigned mask = __ballot_sync(0xffffffffu, pred);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(cnt, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = item;
+}
+
+// block-wide int64 sum (512 threads); result valid in thread 0
+__device__ __forceinline__ long long block_sum64(long long v, long long* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  long long s = 0;
+  if (threadIdx.x < 32) {
+    s = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;
+}
+
+struct SweepShared {
+  int h[HALO];
+  int out[6][TV];
+  long long red[16];
+  int flags;
+};
+
+struct BfsShared {
+  int h[HALO];
+  long long red[16];
+  int flags;
+};
+
+struct ReachShared {
+  unsigned char rc[HALO];
+  unsigned char m[HALO];
+  long long red[16];
+  int flags;
+};
+
+// ---------------------------------------------------------------------------
+// One visit of the push sweep to tile t (L pulses at most).
+//   APPEND: queue the tile itself (if still active) for sweep id_self and the
+//   tiles it pushed into for sweep id_next (persistent schedule); otherwise
+//   only the act[] flags are maintained (host-driven schedule).
+template <bool APPEND>
+__device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShared& S,
+                           const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
+                           const uint32_t id_self, int32_t* list_self, int32_t* cnt_self) {
+  const int l = threadIdx.x;
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  const int64_t g = (int64_t)t * TV + l;
+  const int64_t Np = P.Np;
+  int e = __ldcg(P.e + g), h = __ldcg(P.h + g), rT = __ldcg(P.rT + g);
+  int r[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) r[d] = __ldcg(P.r + d * Np + g);
+  const int hi = halo_index(x, y, z);
+  S.h[hi] = h;
+  load_halo_heights(P, t, S.h);
+  const int inst = __ldcg(P.tinst + t);
+  const int hdead = P.geo[inst].hdead;
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+
+  int acc[6] = {0, 0, 0, 0, 0, 0};  // flow pushed out of the tile, per face
+  int sink = 0;
+  int pulses = 0;
+  for (int p = 0; p < L; ++p) {
+    int hn[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) hn[d] = S.h[hi + hoff(d)];
+    int pushed[6] = {0, 0, 0, 0, 0, 0};
+    if (e > 0 && h < INF) {
+      if (rT > 0 && h == 1) {
+        const int dl = min(e, rT);
+        e -= dl; rT -= dl; sink += dl;
+      }
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (e > 0 && r[d] > 0 && hn[d] == h - 1) {
+          const int dl = min(e, r[d]);
+          e -= dl; r[d] -= dl; pushed[d] = dl;
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      if (inside(d, x, y, z)) S.out[d][l] = pushed[d];
+      else acc[d] += pushed[d];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      if (inside(d, x, y, z)) {
+        const int din = S.out[d ^ 1][l + loff(d)];
+        e += din; r[d] += din;
+      }
+    }
+    int hnew = h;
+    if (e > 0 && h < INF) {
+      bool adm = (rT > 0 && h == 1);
+      int mn = (rT > 0) ? 0 : INF;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (r[d] > 0) { adm = adm || (hn[d] == h - 1); mn = min(mn, hn[d]); }
+      }
+      if (!adm) {
+        hnew = (mn >= INF) ? INF : mn + 1;
+        if (hnew >= hdead) hnew = INF;
+      }
+    }
+    ++pulses;
+    const int any = __syncthreads_or(e > 0 && hnew < INF);
+    h = hnew;
+    S.h[hi] = h;
+    if (!any) break;
+    __syncthreads();
+  }
+
+  // write back the tile
+  P.e[g] = e; P.h[g] = h; P.rT[g] = rT;
+  unsigned m = (rT > 0) ? 64u : 0u;
+#pragma unroll
+  for (int d = 0; d < 6; ++d) { P.r[d * Np + g] = r[d]; m |= (r[d] > 0 ? 1u : 0u) << d; }
+  P.rmask[g] = (uint8_t)m;
+  // flow that left the tile: excess and reverse residual of the neighbour
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    if (!inside(d, x, y, z) && acc[d] > 0) {
+      const int nt = __ldcg(P.nbr + d * P.T + t);
+      if (nt < 0) { raise_error(P, CGC_ERR_OVERFLOW); continue; }  // capacity leaving the grid
+      const int64_t ng = (int64_t)nt * TV + l + xoff(d);
+      atomicAdd(P.e + ng, acc[d]);
+      atomicAdd(P.r + (d ^ 1) * Np + ng, acc[d]);
+      atomicOr((unsigned*)(P.rmask + (ng & ~(int64_t)3)), 1u << (8 * (int)(ng & 3) + (d ^ 1)));
+      atomicOr(&S.flags, 1 << d);
+    }
+  }
+  const int still = __syncthreads_or(e > 0 && h < INF);
+  const long long total = block_sum64((long long)sink, S.red);
+  if (l == 0) {
+    P.act[t] = (uint8_t)(still ? 1 : 0);
+    if (total) atomicAdd(P.flow + inst, (unsigned long long)total);
+    atomicAdd(P.stats + S_TILES_SWEPT, 1ull);
+    atomicAdd(P.stats + S_PULSES, (unsigned long long)pulses);
+    if (APPEND && still) {
+      if (atomicExch(P.stamp_sw + t, id_self) != id_self) list_self[atomicAdd(cnt_self, 1)] = t;
+    }
+  }
+  if (l < 6 && ((S.flags >> l) & 1)) {
+    const int nt = __ldcg(P.nbr + l * P.T + t);
+    P.act[nt] = 1;
+    if (APPEND) {
+      if (atomicExch(P.stamp_sw + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// BFS seed for tile t: h = 1 where the sink residual is positive, INF elsewhere.
+__device__ void bfs_init_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  const int64_t g = (int64_t)t * TV + threadIdx.x;
+  const bool seed = (__ldcg(P.rmask + g) & 64u) != 0;
+  P.h[g] = seed ? 1 : INF;
+  const int any = __syncthreads_or(seed);
+  if (threadIdx.x == 0) {
+    P.act[t] = 0;
+    if (any) {
+      P.stamp_bfs[t] = id0;
+      list0[atomicAdd(cnt0, 1)] = t;
+    }
+  }
+}
+
+// One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
+// until the tile is stable; re-queue face neighbours whose halo changed.
+__device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
+                         int32_t* list_next, int32_t* cnt_next) {
+  const int l = threadIdx.x;
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  const int64_t g = (int64_t)t * TV + l;
+  int h = __ldcg(P.h + g);
+  const int h0 = h;
+  const unsigned m = __ldcg(P.rmask + g);
+  const int e = __ldcg(P.e + g);
+  const int hi = halo_index(x, y, z);
+  S.h[hi] = h;
+  load_halo_heights(P, t, S.h);
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+  for (int it = 0; it < 1024; ++it) {  // converges in < 512 steps (path length in a tile)
+    int mn = h;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+      if ((m >> d) & 1u) mn = min(mn, S.h[hi + hoff(d)] + 1);
+    const bool ch = mn < h;
+    const int any = __syncthreads_or(ch);
+    if (!any) break;
+    if (ch) { h = mn; S.h[hi] = h; }
+    __syncthreads();
+  }
+  if (h < h0) {
+    P.h[g] = h;
+    const int fb = face_bits(x, y, z);
+    if (fb) atomicOr(&S.flags, fb);
+  }
+  const int act = __syncthreads_or(e > 0 && h < INF);
+  if (l == 0) {
+    P.act[t] = (uint8_t)(act ? 1 : 0);
+    atomicAdd(P.stats + S_TILES_BFS, 1ull);
+  }
+  if (l < 6 && ((S.flags >> l) & 1)) {
+    const int nt = __ldcg(P.nbr + l * P.T + t);
+    if (nt >= 0 && atomicExch(P.stamp_bfs + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Source-side reachability (canonical cut) after the maximum preflow:
+// closure of {v : e(v) > 0} over residual edges.
+__device__ void reach_init_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  const int64_t g = (int64_t)t * TV + threadIdx.x;
+  const bool seed = __ldcg(P.e + g) > 0;
+  P.reach[g] = seed ? 1 : 0;
+  const int any = __syncthreads_or(seed);
+  if (threadIdx.x == 0 && any) {
+    P.stamp_bfs[t] = id0;
+    list0[atomicAdd(cnt0, 1)] = t;
+  }
+}
+
+__device__ void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
+                           int32_t* list_next, int32_t* cnt_next) {
+  const int l = threadIdx.x;
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  const int64_t g = (int64_t)t * TV + l;
+  int rc = __ldcg(P.reach + g);
+  const int rc0 = rc;
+  const int hi = halo_index(x, y, z);
+  S.rc[hi] = (unsigned char)rc;
+  S.m[hi] = __ldcg(P.rmask + g);
+  for_halo_entry(l, [&](int f, int hh, int src) {
+    const int nt = __ldcg(P.nbr + f * P.T + t);
+    if (nt >= 0) {
+      S.rc[hh] = __ldcg(P.reach + (int64_t)nt * TV + src);
+      S.m[hh] = __ldcg(P.rmask + (int64_t)nt * TV + src);
+    } else {
+      S.rc[hh] = 0; S.m[hh] = 0;
+    }
+  });
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+  for (int it = 0; it < 1024; ++it) {
+    bool ch = false;
+    if (!rc) {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        const int u = hi + hoff(d);
+        if (S.rc[u] && ((S.m[u] >> (d ^ 1)) & 1u)) ch = true;
+      }
+    }
+    const int any = __syncthreads_or(ch);
+    if (!any) break;
+    if (ch) { rc = 1; S.rc[hi] = 1; }
+    __syncthreads();
+  }
+  if (rc && !rc0) {
+    P.reach[g] = 1;
+    const int fb = face_bits(x, y, z);
+    if (fb) atomicOr(&S.flags, fb);
+  }
+  __syncthreads();
+  if (l < 6 && ((S.flags >> l) & 1)) {
+    const int nt = __ldcg(P.nbr + l * P.T + t);
+    if (nt >= 0 && atomicExch(P.stamp_bfs + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
+  }
+  __syncthreads();
+}
+
+}  // namespace cgc

@@ -1,0 +1,282 @@
+"""Host-side mirror of cugip's graph-cut interface over the C ABI of libcgc.
+
+`Graph` keeps the names, argument meaning and error behaviour of
+`cugip::Graph<TFlow>` (include/cugip/advanced_operations/graph_cut.hpp:47-146):
+set_vertex_count / set_nweights(edge list) / set_tweights / max_flow /
+fill_segments, with int32 capacities and an exact int flow.  `GridGraph` is
+the grid-native form: t-link volumes and one n-link volume per axis, which is
+what the reference's grid front-end builds
+(benchmarks/graph_cut/graph_cut.cpp:33-98).  `Batch` solves many grids of
+uneven sizes in one launch.
+
+Every solve runs on the GPU through libcgc.so; nothing here computes a flow.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import CgcError, check
+
+SINK = "sink"      # vertices that can reach the sink (reference fill_segments semantics)
+SOURCE = "source"  # vertices reachable from the source (minimal source side: the canonical cut)
+
+
+def _which(which: str) -> int:
+    if which in (SINK, _lib.SEG_SINK_REACH):
+        return _lib.SEG_SINK_REACH
+    if which in (SOURCE, _lib.SEG_SOURCE_MIN):
+        return _lib.SEG_SOURCE_MIN
+    raise ValueError(f"unknown segment set {which!r}")
+
+
+def _i32(a, n: int, name: str) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a).reshape(-1))
+    if arr.dtype != np.int32:
+        if arr.dtype.kind == "f":
+            if not np.all(np.isfinite(arr)) or not np.all(arr == np.round(arr)):
+                raise CgcError(1, f"{name}: capacities must be integral (the engine is exact)")
+        if arr.size and (arr.min() < 0 or arr.max() > np.iinfo(np.int32).max):
+            raise CgcError(1, f"{name}: capacities must be in [0, 2^31)")
+        arr = arr.astype(np.int32)
+    if arr.size != n:
+        raise CgcError(1, f"{name}: expected {n} entries, got {arr.size}")
+    return arr
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Policy:
+    """Runtime counterpart of GraphCutPolicy (detail/graph_cut_policies.hpp:23-89)."""
+
+    def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0,
+                 max_sweeps: int = 0, persistent: int = 0):
+        self.local_pulses = local_pulses
+        self.sweeps_per_relabel = sweeps_per_relabel
+        self.schedule = schedule
+        self.max_sweeps = max_sweeps
+        self.persistent = persistent
+
+    def options(self) -> _lib.Options:
+        return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
+                            self.persistent)
+
+
+class GridGraph:
+    """X*Y*Z 6-connected grid graph; vertex id = x + X*(y + Y*z)."""
+
+    def __init__(self, X: int, Y: int, Z: int = 1, stream: int | None = None):
+        self._lib = _lib.load()
+        self.X, self.Y, self.Z = int(X), int(Y), int(Z)
+        self.n = self.X * self.Y * self.Z
+        h = C.c_void_p()
+        check(self._lib.cgc_grid_create(self.X, self.Y, self.Z, C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self.flow: int | None = None
+
+    @classmethod
+    def _wrap(cls, handle: C.c_void_p, dims) -> "GridGraph":
+        g = cls.__new__(cls)
+        g._lib = _lib.load()
+        g.X, g.Y, g.Z = (int(d) for d in dims)
+        g.n = g.X * g.Y * g.Z
+        g._h = handle
+        g.flow = None
+        return g
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cgc_grid_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- capacities ---------------------------------------------------------
+    def set_tweights(self, cap_source, cap_sink) -> None:
+        s = _i32(cap_source, self.n, "cap_source")
+        t = _i32(cap_sink, self.n, "cap_sink")
+        check(self._lib.cgc_grid_set_tlinks(self._h, _ptr(s), _ptr(t)))
+
+    def set_nweights(self, axis: int, forward, backward=None) -> None:
+        """n-links along `axis` (0=x,1=y,2=z): forward[v] = cap v -> v+e_axis,
+        backward[v] = cap v+e_axis -> v (same as forward when omitted)."""
+        f = _i32(forward, self.n, "forward")
+        b = f if backward is None else _i32(backward, self.n, "backward")
+        check(self._lib.cgc_grid_set_nlinks(self._h, int(axis), _ptr(f), _ptr(b)))
+
+    def set_tweights_device(self, cap_source_ptr: int, cap_sink_ptr: int) -> None:
+        check(self._lib.cgc_grid_set_tlinks_device(self._h, C.c_void_p(cap_source_ptr), C.c_void_p(cap_sink_ptr)))
+
+    def set_nweights_device(self, axis: int, forward_ptr: int, backward_ptr: int | None = None) -> None:
+        b = forward_ptr if backward_ptr is None else backward_ptr
+        check(self._lib.cgc_grid_set_nlinks_device(self._h, int(axis), C.c_void_p(forward_ptr), C.c_void_p(b)))
+
+    # -- solve --------------------------------------------------------------
+    def max_flow(self, policy: Policy | None = None) -> int:
+        flow = C.c_int64()
+        opts = policy.options() if policy else None
+        check(self._lib.cgc_grid_maxflow(self._h, C.byref(opts) if opts else None, C.byref(flow)))
+        self.flow = int(flow.value)
+        return self.flow
+
+    def fill_segments(self, out: np.ndarray | None = None, mask: int = 255, background: int = 0,
+                      which: str = SINK) -> np.ndarray:
+        """out[v] = mask where v is in the chosen set, else background.
+        which=SINK: vertices that can reach the sink (cugip's fill_segments,
+        graph_cut.hpp:304-333); which=SOURCE: vertices reachable from the source
+        (the canonical minimum cut)."""
+        if out is None:
+            out = np.empty(self.n, dtype=np.uint8)
+        if out.dtype != np.uint8 or not out.flags["C_CONTIGUOUS"] or out.size != self.n:
+            raise CgcError(1, "fill_segments: out must be a contiguous uint8 array of n entries")
+        check(self._lib.cgc_grid_get_segments(self._h, _which(which), _ptr(out), mask, background))
+        return out
+
+    def fill_segments_device(self, out_ptr: int, mask: int = 255, background: int = 0, which: str = SINK) -> None:
+        check(self._lib.cgc_grid_get_segments_device(self._h, _which(which), C.c_void_p(out_ptr), mask, background))
+
+    def residuals(self) -> dict:
+        """Final residual capacities in linear layout: r (6,n) for +x,-x,+y,-y,+z,-z, resT and excess."""
+        r = np.empty((6, self.n), dtype=np.int32)
+        rt = np.empty(self.n, dtype=np.int32)
+        ex = np.empty(self.n, dtype=np.int32)
+        ptrs = (C.c_void_p * 6)(*[r[d].ctypes.data for d in range(6)])
+        check(self._lib.cgc_grid_get_residuals(self._h, ptrs, _ptr(rt), _ptr(ex)))
+        return {"r": r, "resT": rt, "excess": ex}
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(self._lib.cgc_grid_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+
+class Graph:
+    """Mirror of cugip::Graph<TFlow> (graph_cut.hpp:47-146) for int32 capacities.
+
+    Edges are EdgeRecord(first, second) pairs with forward = cap first->second
+    and backward = cap second->first.  The edge list must describe a
+    6-connected grid with linear vertex ids (see cgc_grid_create_from_edges);
+    other graphs raise CgcError(CGC_ERR_NOT_GRID).
+    """
+
+    def __init__(self):
+        self._n = 0
+        self._grid: GridGraph | None = None
+        self._pending_t = None
+
+    def set_vertex_count(self, count: int) -> None:
+        self._n = int(count)
+        self._grid = None
+
+    def set_nweights(self, edge_count: int, edges, weights_forward, weights_backward) -> None:
+        e = np.ascontiguousarray(np.asarray(edges, dtype=np.int64).reshape(-1, 2)[:edge_count])
+        a = np.ascontiguousarray(e[:, 0].astype(np.uint32))
+        b = np.ascontiguousarray(e[:, 1].astype(np.uint32))
+        f = _i32(np.asarray(weights_forward)[:edge_count], edge_count, "weights_forward")
+        w = _i32(np.asarray(weights_backward)[:edge_count], edge_count, "weights_backward")
+        h = C.c_void_p()
+        dims = (C.c_int32 * 3)()
+        lib = _lib.load()
+        check(lib.cgc_grid_create_from_edges(self._n, edge_count, _ptr(a), _ptr(b), _ptr(f), _ptr(w),
+                                             None, C.byref(h), dims))
+        self._grid = GridGraph._wrap(h, list(dims))
+        if self._pending_t is not None:
+            self._grid.set_tweights(*self._pending_t)
+            self._pending_t = None
+
+    def set_tweights(self, cap_source, cap_sink) -> None:
+        if self._grid is None:
+            # the reference allows t-links before n-links; keep them until the grid exists
+            self._pending_t = (_i32(cap_source, self._n, "cap_source"), _i32(cap_sink, self._n, "cap_sink"))
+            return
+        self._grid.set_tweights(cap_source, cap_sink)
+
+    def max_flow(self, policy: Policy | None = None) -> int:
+        if self._grid is None:
+            raise CgcError(7, "max_flow: set_nweights was not called")
+        return self._grid.max_flow(policy)
+
+    def fill_segments(self, out=None, mask: int = 255, background: int = 0, which: str = SINK):
+        if self._grid is None:
+            raise CgcError(7, "fill_segments: no graph")
+        seg = self._grid.fill_segments(None, mask, background, which)
+        if out is None:
+            return seg
+        out[...] = seg.reshape(np.shape(out))
+        return out
+
+    @property
+    def grid(self) -> GridGraph | None:
+        return self._grid
+
+
+class Batch:
+    """Many grid instances of uneven sizes solved by one launch."""
+
+    def __init__(self, extents: Sequence[Sequence[int]], stream: int | None = None):
+        self._lib = _lib.load()
+        ext = np.ascontiguousarray(np.asarray(extents, dtype=np.int32).reshape(-1, 3))
+        self.extents = [tuple(int(v) for v in row) for row in ext]
+        h = C.c_void_p()
+        check(self._lib.cgc_batch_create(len(self.extents), _ptr(ext), C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self.flows: list[int] | None = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cgc_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _n(self, i: int) -> int:
+        X, Y, Z = self.extents[i]
+        return X * Y * Z
+
+    def set_tweights(self, i: int, cap_source, cap_sink) -> None:
+        n = self._n(i)
+        check(self._lib.cgc_batch_set_tlinks(self._h, i, _ptr(_i32(cap_source, n, "cap_source")),
+                                             _ptr(_i32(cap_sink, n, "cap_sink"))))
+
+    def set_nweights(self, i: int, axis: int, forward, backward=None) -> None:
+        n = self._n(i)
+        f = _i32(forward, n, "forward")
+        b = f if backward is None else _i32(backward, n, "backward")
+        check(self._lib.cgc_batch_set_nlinks(self._h, i, int(axis), _ptr(f), _ptr(b)))
+
+    def max_flow(self, policy: Policy | None = None) -> list[int]:
+        flows = np.zeros(len(self.extents), dtype=np.int64)
+        opts = policy.options() if policy else None
+        check(self._lib.cgc_batch_maxflow(self._h, C.byref(opts) if opts else None,
+                                          flows.ctypes.data_as(_lib.P64)))
+        self.flows = [int(f) for f in flows]
+        return self.flows
+
+    def fill_segments(self, i: int, mask: int = 255, background: int = 0, which: str = SINK) -> np.ndarray:
+        out = np.empty(self._n(i), dtype=np.uint8)
+        check(self._lib.cgc_batch_get_segments(self._h, i, _which(which), _ptr(out), mask, background))
+        return out
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(self._lib.cgc_batch_stats(self._h, C.byref(s)))
+        return s.as_dict()

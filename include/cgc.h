@@ -1,0 +1,211 @@
+/*
+ * cgc.h — C ABI of the B200 grid graph-cut (max-flow / min-cut) engine.
+ *
+ * Plain pointers and sizes only; every entry point returns an int status
+ * (CGC_OK == 0).  The message of the last failure on the calling thread is
+ * returned by cgc_last_error().
+ *
+ * Each entry point names the interface of cugip's graph-cut path that it
+ * replaces (paths relative to the cugip source tree).
+ *
+ * Graph model (identical to cugip::Graph<TFlow>):
+ *   - one vertex per voxel, vertex id = x + X*(y + Y*z) (x fastest);
+ *   - a t-link from the source with capacity capS[v] and one to the sink
+ *     with capacity capT[v]  (include/cugip/advanced_operations/graph_cut.hpp:64-67);
+ *   - an n-link between each pair of 6-neighbours with a forward capacity
+ *     (lower id -> higher id) and a backward capacity (higher -> lower),
+ *     the EdgeRecord(min,max) + fwd/bwd convention of
+ *     include/cugip/advanced_operations/graph_cut.hpp:57-62 and
+ *     include/cugip/advanced_operations/detail/edge_record.hpp:12-17.
+ * Capacities are int32 >= 0; the flow value is returned as int64 and is exact.
+ */
+#ifndef CGC_H
+#define CGC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  CGC_OK = 0,
+  CGC_ERR_ARG = 1,           /* bad argument (null pointer, bad extent, bad axis) */
+  CGC_ERR_OOM = 2,           /* device or host allocation failed                  */
+  CGC_ERR_CUDA = 3,          /* a CUDA runtime call failed                         */
+  CGC_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up                 */
+  CGC_ERR_NOT_CONVERGED = 5, /* max_sweeps reached before the max flow was proven  */
+  CGC_ERR_OVERFLOW = 6,      /* capacities could overflow the int32 residual/excess range */
+  CGC_ERR_STATE = 7,         /* call out of order (e.g. segments before max_flow)  */
+  CGC_ERR_NOT_GRID = 8,      /* edge list is not a 6-connected grid                */
+  CGC_ERR_NO_DEVICE = 9      /* no CUDA device                                     */
+};
+
+/* axes for cgc_grid_set_nlinks */
+enum { CGC_AXIS_X = 0, CGC_AXIS_Y = 1, CGC_AXIS_Z = 2 };
+
+/* which labelling cgc_grid_get_segments returns */
+enum {
+  /* vertices that can reach the sink in the final residual graph: the set
+     cugip marks with label in [0, n] (graph_cut.hpp:304-333) and the set
+     Boykov-Kolmogorov's what_segment()==SINK returns
+     (benchmarks/graph_cut/boykov_kolmogorov.cpp:81) */
+  CGC_SEG_SINK_REACH = 0,
+  /* vertices reachable from the source in the final residual graph: the
+     minimal source side of the minimum cut (the canonical cut) */
+  CGC_SEG_SOURCE_MIN = 1
+};
+
+/* schedules of the tile sweep */
+enum {
+  CGC_SCHED_PARITY = 0, /* checkerboard tiles: halo heights exact, deterministic */
+  CGC_SCHED_ASYNC = 1   /* all active tiles each sweep, stale halo heights      */
+};
+
+/* Solver options; zero-initialise and set struct_size = sizeof(cgc_options).
+   A zero field means "use the default".  Replaces the compile-time policies
+   GraphCutPolicy / RelabelPolicy / PushPolicy
+   (include/cugip/advanced_operations/detail/graph_cut_policies.hpp:23-89). */
+typedef struct cgc_options {
+  int32_t struct_size;
+  int32_t local_pulses;       /* push/relabel pulses per tile visit (1..64), default 16 */
+  int32_t sweeps_per_relabel; /* sweep pairs between global relabels, default 8 */
+  int32_t schedule;           /* CGC_SCHED_* (default parity) */
+  int32_t max_sweeps;         /* safety cap on sweep pairs, default 1<<20 */
+  int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
+  int32_t reserved[10];
+} cgc_options;
+
+/* Per-solve statistics (filled by cgc_grid_stats). */
+typedef struct cgc_stats {
+  int64_t flow;
+  int64_t sweeps;            /* parity sweeps executed */
+  int64_t global_relabels;   /* exact BFS relabels executed */
+  int64_t bfs_rounds;        /* tile rounds over all BFS passes */
+  int64_t tiles_swept;       /* tile visits by the push sweep */
+  int64_t tiles_relabelled;  /* tile visits by the BFS */
+  int64_t pulses;            /* total local pulses executed over all tile visits */
+  double  solve_ms;          /* device time of the last maxflow (preparation + solve) */
+  double  kernel_ms;         /* device time of the solve kernel(s) alone */
+  int64_t launches;          /* kernels launched by the last maxflow */
+  int64_t reserved[6];
+} cgc_stats;
+
+/* Kernels launched by this library on the calling process since load
+ * (uploads, solve, outputs): for launch accounting in benchmarks. */
+int64_t cgc_launch_count(void);
+
+typedef struct cgc_grid cgc_grid;
+
+/* ---- library ------------------------------------------------------------ */
+const char* cgc_last_error(void);
+const char* cgc_version(void);
+/* Initialises the CUDA device and returns CGC_ERR_NO_DEVICE without one. */
+int cgc_init(int device);
+
+/* ---- single grid ---------------------------------------------------------
+ * Replaces cugip::Graph<TFlow>::set_vertex_count
+ * (include/cugip/advanced_operations/graph_cut.hpp:213-237): allocates all
+ * device state for an X*Y*Z grid (about 40 bytes per voxel, padded to 8^3
+ * tiles).  stream may be NULL (legacy default stream). */
+int cgc_grid_create(int32_t X, int32_t Y, int32_t Z, void* stream, cgc_grid** out);
+int cgc_grid_destroy(cgc_grid* g);
+
+/* Replaces Graph::set_tweights (graph_cut.hpp:292-302).  Host arrays of X*Y*Z
+ * int32 >= 0, copied to the device before the call returns. */
+int cgc_grid_set_tlinks(cgc_grid* g, const int32_t* capS, const int32_t* capT);
+
+/* Replaces Graph::set_nweights (graph_cut.hpp:239-290) for a grid: the n-links
+ * along one axis.  fwd[v] is the capacity v -> v+e_axis, bwd[v] the capacity
+ * v+e_axis -> v; entries on the last slice of the axis are ignored.  When
+ * fwd == bwd (symmetric weights) the plane is copied once. Host arrays. */
+int cgc_grid_set_nlinks(cgc_grid* g, int axis, const int32_t* fwd, const int32_t* bwd);
+
+/* Edge-list front door, replacing Graph::set_vertex_count + set_nweights
+ * (graph_cut.hpp:213-290) for callers that build EdgeRecord lists: edge i
+ * joins vertices a[i] and b[i] with capacity fwd[i] from a[i] to b[i] and
+ * bwd[i] from b[i] to a[i] (for EdgeRecord(first,second), pass first/second).
+ * The edges must form a 6-connected X*Y*Z grid with linear ids (x fastest);
+ * the extents are recovered from the id strides, written to dims_out (may be
+ * NULL) and the n-links are uploaded.  Parallel edges add up.  Returns
+ * CGC_ERR_NOT_GRID for any other graph. */
+int cgc_detect_grid(int32_t n, int64_t m, const uint32_t* a, const uint32_t* b, int32_t* dims);
+int cgc_grid_create_from_edges(int32_t n, int64_t m, const uint32_t* a, const uint32_t* b,
+                               const int32_t* fwd, const int32_t* bwd, void* stream, cgc_grid** out,
+                               int32_t* dims_out);
+
+/* Same as the two setters above with device pointers (no host copies). */
+int cgc_grid_set_tlinks_device(cgc_grid* g, const int32_t* capS, const int32_t* capT);
+int cgc_grid_set_nlinks_device(cgc_grid* g, int axis, const int32_t* fwd, const int32_t* bwd);
+
+/* Replaces Graph::max_flow / max_flow(policy)
+ * (graph_cut.hpp:69-100 -> MinimalGraphCutComputation::run,
+ * detail/graph_cut_implementation.hpp:286-308).  Runs push-relabel to the
+ * exact maximum flow; *flow receives the int64 flow value.  opts may be NULL.
+ * Blocks until done.  Unlike the reference, the graph may be solved again
+ * after new set_* calls. */
+int cgc_grid_maxflow(cgc_grid* g, const cgc_options* opts, int64_t* flow);
+
+/* Replaces Graph::fill_segments (graph_cut.hpp:318-333): out[v] = mask if v is
+ * in the chosen set (CGC_SEG_*), else background.  Host array of X*Y*Z. */
+int cgc_grid_get_segments(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background);
+/* Same into device memory. */
+int cgc_grid_get_segments_device(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background);
+
+/* Final residual capacities (host arrays of X*Y*Z each, linear layout):
+ * res[d] for d = +x,-x,+y,-y,+z,-z (entries that leave the grid are 0), the
+ * sink t-link residual resT and the excess left at each voxel.  For
+ * certificates and tests; any pointer may be NULL. */
+int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, int32_t* excess);
+
+int cgc_grid_stats(cgc_grid* g, cgc_stats* out);
+
+/* ---- batch of grids (uneven sizes, one solve) ----------------------------
+ * Replaces nothing in the reference (it solves one graph per Graph object);
+ * all instances share one tile pool and are solved by the same launches. */
+typedef struct cgc_batch cgc_batch;
+int cgc_batch_create(int32_t count, const int32_t* extents /* 3*count: X,Y,Z */, void* stream, cgc_batch** out);
+int cgc_batch_destroy(cgc_batch* b);
+int cgc_batch_set_tlinks(cgc_batch* b, int32_t i, const int32_t* capS, const int32_t* capT);
+int cgc_batch_set_nlinks(cgc_batch* b, int32_t i, int axis, const int32_t* fwd, const int32_t* bwd);
+int cgc_batch_maxflow(cgc_batch* b, const cgc_options* opts, int64_t* flows /* count */);
+int cgc_batch_get_segments(cgc_batch* b, int32_t i, int which, uint8_t* out, uint8_t mask, uint8_t background);
+int cgc_batch_stats(cgc_batch* b, cgc_stats* out);
+
+/* ---- synthetic inputs ------------------------------------------------------
+ * Deterministic capacity volumes for the benchmark workloads (x-fastest,
+ * int32): Gaussian spheres (a ball of radius r whose boundary is blurred by a
+ * Gaussian of edge_sigma voxels: I = bg + (I_obj-bg)*erfc((d-r)/(sqrt2*sigma))/2)
+ * or tubes on a background, Gaussian noise, two-class Gaussian likelihood t-links capS = round(s*(-log p_bg)),
+ * capT = round(s*(-log p_fg)) and contrast n-links
+ * round(w*exp(-(Ii-Ij)^2/(2*sigma^2))).  nx/ny/nz hold the symmetric n-link
+ * to the +x/+y/+z neighbour (0 on the last slice). */
+typedef struct cgc_volume_spec {
+  int32_t X, Y, Z;
+  int32_t kind;              /* 0 = spheres, 1 = tubes */
+  uint64_t seed;
+  int32_t count;             /* spheres or tubes */
+  int32_t n_fixed_radii;     /* spheres: if > 0 use fixed_radii[0..count) */
+  double fixed_radii[8];
+  double radius_min, radius_max;
+  double intensity_min, intensity_max;
+  double background, noise_sd;
+  double mu_bg, mu_fg, class_sd;
+  double tlink_scale, nlink_scale, nlink_sigma;
+  int32_t ctrl_min, ctrl_max; /* tubes: control points per spline */
+  double edge_sigma;         /* spheres: Gaussian blur of the boundary (voxels), 0 = hard edge */
+} cgc_volume_spec;
+
+/* Fills the spec of a named workload: which = 1 (64^3 two spheres),
+ * 2 (256^3 40 spheres), 3 (512x512x128 200 tubes), 4 (batched instance
+ * `index`, extents in 32..160), 5 (128^3 training instance `index`). */
+int cgc_volume_preset(int which, int32_t index, cgc_volume_spec* out);
+int cgc_volume_generate(const cgc_volume_spec* spec, int32_t* capS, int32_t* capT,
+                        int32_t* nx, int32_t* ny, int32_t* nz, float* image /* may be NULL */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGC_H */

@@ -1,0 +1,168 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle and the
+golden fixtures -- exact flow value and bit-identical cut sets."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cugip_b200 import _lib, volume
+from cugip_b200.graph_cut import SINK, SOURCE, Batch, Graph, GridGraph, Policy
+from oracle import oracle
+from tests import graphs
+from tests.gpu_helpers import certify, sha, solve
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.json")))
+CASES = {(c["workload"], c["index"]): c for c in GOLDEN["cases"]}
+
+POLICIES = {
+    "default": None,
+    "host_loop": Policy(persistent=-1),
+    "L1_K1": Policy(local_pulses=1, sweeps_per_relabel=1),
+    "L4_K2": Policy(local_pulses=4, sweeps_per_relabel=2),
+    "L32_K32": Policy(local_pulses=32, sweeps_per_relabel=32),
+    "host_L2": Policy(local_pulses=2, sweeps_per_relabel=3, persistent=-1),
+}
+
+
+def test_reference_four_by_four_through_graph_api():
+    n, a, b, f, g, s, t = graphs.four_by_four()
+    G = Graph()
+    G.set_vertex_count(n)
+    G.set_tweights(s.astype(np.float32), t.astype(np.float32))  # reference tests pass float weights
+    G.set_nweights(len(a), np.stack([a, b], 1), f.astype(np.float32), g.astype(np.float32))
+    assert G.max_flow() == 4
+    out = np.zeros(16, np.uint8)
+    G.fill_segments(out)  # default mask 255 / background 0: sink-reachable vertices
+    assert out.tolist() == [0] * 8 + [255] * 8
+    assert G.fill_segments(mask=1, which=SOURCE).tolist() == [1] * 8 + [0] * 8
+
+
+def test_layered_reference_graph_is_rejected_loudly():
+    n, a, b, f, g, s, t = graphs.layered(layers=6, size=32, nbrs=4)
+    G = Graph()
+    G.set_vertex_count(n)
+    with pytest.raises(_lib.CgcError) as e:
+        G.set_nweights(len(a), np.stack([a, b], 1), f, g)
+    assert e.value.code == 8
+
+
+@pytest.mark.parametrize("policy", list(POLICIES))
+@pytest.mark.parametrize("dims,seed", [((8, 8, 8), 1), ((7, 5, 3), 2), ((16, 16, 4), 3), ((9, 1, 1), 4),
+                                       ((33, 17, 9), 5), ((64, 8, 8), 6), ((20, 20, 20), 7), ((1, 1, 1), 8),
+                                       ((40, 3, 17), 9)])
+def test_random_grids_match_oracle(dims, seed, policy):
+    X, Y, Z = dims
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, seed)
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    flow, smin, treach, st, res = solve(X, Y, Z, capS, capT, fwd, bwd, POLICIES[policy], residuals=True)
+    assert flow == f0
+    assert np.array_equal(smin, s0)
+    assert np.array_equal(treach, t0)
+    certify(X, Y, Z, capS, capT, fwd, bwd, flow, res, smin, treach)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_long_paths_match_oracle(seed):
+    """Sparse capacities: long thin augmenting paths (many BFS rounds, many sweeps)."""
+    X, Y, Z = 48, 40, 24
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, 100 + seed, tmax=30, nmax=20, zero_frac=0.9)
+    for f in fwd + bwd:
+        f[np.random.default_rng(seed).random(f.size) < 0.4] = 0
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    for pol in (None, Policy(persistent=-1)):
+        flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, bwd, pol)
+        assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
+
+
+@pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 4, 5)])
+def test_golden_workloads(key):
+    c = CASES[key]
+    v = volume.workload(*key)
+    assert sha(*v.arrays()) == c["volume_sha256"]
+    flow, smin, treach, st = solve(v.X, v.Y, v.Z, v.capS, v.capT, v.n)
+    assert flow == c["flow"]
+    assert sha(smin) == c["smin_sha256"]
+    assert sha(treach) == c["treach_sha256"]
+
+
+@pytest.mark.parametrize("key", [(2, 0), (3, 0)])
+def test_full_size_workloads_with_certificate(key):
+    c = CASES[key]
+    v = volume.workload(*key)
+    flow, smin, treach, st, res = solve(v.X, v.Y, v.Z, v.capS, v.capT, v.n, residuals=True)
+    assert flow == c["flow"]
+    assert sha(smin) == c["smin_sha256"] and sha(treach) == c["treach_sha256"]
+    certify(v.X, v.Y, v.Z, v.capS, v.capT, v.n, None, flow, res, smin, treach)
+
+
+def test_batch_matches_golden():
+    keys = [(4, i) for i in range(8)]
+    vols = [volume.workload(*k) for k in keys]
+    B = Batch([(v.X, v.Y, v.Z) for v in vols])
+    for i, v in enumerate(vols):
+        B.set_tweights(i, v.capS, v.capT)
+        for ax in range(3):
+            B.set_nweights(i, ax, v.n[ax])
+    flows = B.max_flow()
+    for i, k in enumerate(keys):
+        c = CASES[k]
+        assert flows[i] == c["flow"]
+        assert sha(B.fill_segments(i, mask=1, which=SOURCE)) == c["smin_sha256"]
+        assert sha(B.fill_segments(i, mask=1, which=SINK)) == c["treach_sha256"]
+    B.close()
+
+
+def test_edge_cases():
+    # all zero: nothing flows, nothing reachable
+    X, Y, Z = 10, 9, 3
+    N = X * Y * Z
+    z = np.zeros(N, np.int32)
+    flow, smin, treach, _ = solve(X, Y, Z, z, z, [z, z, z])
+    assert flow == 0 and smin.sum() == 0 and treach.sum() == 0
+    # t-links only: flow is the sum of min(capS, capT)
+    rng = np.random.default_rng(0)
+    s, t = rng.integers(0, 50, N).astype(np.int32), rng.integers(0, 50, N).astype(np.int32)
+    flow, smin, treach, _ = solve(X, Y, Z, s, t, [z, z, z])
+    assert flow == int(np.minimum(s, t).sum())
+    assert np.array_equal(smin.astype(bool), s > t) and np.array_equal(treach.astype(bool), t > s)
+
+
+def test_errors_are_loud():
+    X, Y, Z = 8, 8, 8
+    N = X * Y * Z
+    g = GridGraph(X, Y, Z)
+    with pytest.raises(_lib.CgcError) as e:
+        g.fill_segments()
+    assert e.value.code == 7  # CGC_ERR_STATE before max_flow
+    with pytest.raises(_lib.CgcError) as e:
+        g.max_flow()
+    assert e.value.code == 7  # no t-links yet
+    big = np.full(N, 2**31 - 1, np.int32)
+    g.set_tweights(big, np.zeros(N, np.int32))
+    for ax in range(3):
+        g.set_nweights(ax, big)
+    with pytest.raises(_lib.CgcError) as e:
+        g.max_flow()
+    assert e.value.code == 6  # CGC_ERR_OVERFLOW
+    g.close()
+
+
+def test_resolve_after_reupload_is_identical():
+    X, Y, Z = 24, 16, 12
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, 77)
+    g = GridGraph(X, Y, Z)
+    res = []
+    for _ in range(3):
+        g.set_tweights(capS, capT)
+        for ax in range(3):
+            g.set_nweights(ax, fwd[ax], bwd[ax])
+        res.append((g.max_flow(), sha(g.fill_segments(which=SOURCE)), sha(g.fill_segments(which=SINK))))
+    with pytest.raises(_lib.CgcError):
+        g.max_flow()  # capacities were consumed by the last solve
+    g.close()
+    assert res[0] == res[1] == res[2]
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    assert res[0][0] == f0
