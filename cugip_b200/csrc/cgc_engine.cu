@@ -168,7 +168,8 @@ __global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
 }
 
 __global__ void __launch_bounds__(512) k_bfs_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
-  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, id0, list0, cnt0);
+  __shared__ BfsShared S;
+  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, S, id0, list0, cnt0);
 }
 
 __global__ void __launch_bounds__(512, 2) k_bfs_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
@@ -179,7 +180,8 @@ __global__ void __launch_bounds__(512, 2) k_bfs_round(DevPool P, const int32_t* 
 }
 
 __global__ void __launch_bounds__(512) k_reach_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
-  for (int t = blockIdx.x; t < P.T; t += gridDim.x) reach_init_tile(P, t, id0, list0, cnt0);
+  __shared__ ReachShared S;
+  for (int t = blockIdx.x; t < P.T; t += gridDim.x) reach_init_tile(P, t, S, id0, list0, cnt0);
 }
 
 __global__ void __launch_bounds__(512, 2) k_reach_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
       sc[0] = sc[1] = sc[2] = sc[3] = 0;
     }
     if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, bfs_id, bl[0], bc + 0);
+    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs, bfs_id, bl[0], bc + 0);
     if (!grid_sync(P, prm.limit_ns)) return;
     int k = 0;
     for (;;) {
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   // ------------------------------------------------ source-side reachability
   if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
   if (!grid_sync(P, prm.limit_ns)) return;
-  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, bfs_id, bl[0], bc + 0);
+  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, S.rc, bfs_id, bl[0], bc + 0);
   if (!grid_sync(P, prm.limit_ns)) return;
   int k = 0;
   for (;;) {

@@ -261,18 +261,36 @@ __device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShar
 
 // ---------------------------------------------------------------------------
 // BFS seed for tile t: h = 1 where the sink residual is positive, INF elsewhere.
-__device__ void bfs_init_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0, int32_t* cnt0) {
-  const int64_t g = (int64_t)t * TV + threadIdx.x;
+// A tile with seeds is queued, and so is every face neighbour next to a seed
+// on the tile's face (the neighbour reads the seed through its halo).
+__device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
+                                           int32_t* cnt) {
+  if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
+}
+
+__device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id0, int32_t* list0,
+                              int32_t* cnt0) {
+  const int l = threadIdx.x;
+  const int64_t g = (int64_t)t * TV + l;
   const bool seed = (__ldcg(P.rmask + g) & 64u) != 0;
   P.h[g] = seed ? 1 : INF;
-  const int any = __syncthreads_or(seed);
-  if (threadIdx.x == 0) {
-    P.act[t] = 0;
-    if (any) {
-      P.stamp_bfs[t] = id0;
-      list0[atomicAdd(cnt0, 1)] = t;
-    }
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+  if (seed) {
+    const int fb = face_bits(l & 7, (l >> 3) & 7, l >> 6);
+    atomicOr(&S.flags, fb | 64);
   }
+  __syncthreads();
+  const int fl = S.flags;
+  if (l == 0) {
+    P.act[t] = 0;
+    if (fl & 64) queue_tile(P, P.stamp_bfs, t, id0, list0, cnt0);
+  }
+  if (l < 6 && ((fl >> l) & 1)) {
+    const int nt = __ldcg(P.nbr + l * P.T + t);
+    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id0, list0, cnt0);
+  }
+  __syncthreads();
 }
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
@@ -314,7 +332,7 @@ __device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint
   }
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0 && atomicExch(P.stamp_bfs + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
+    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id_next, list_next, cnt_next);
   }
   __syncthreads();
 }
@@ -322,15 +340,26 @@ __device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint
 // ---------------------------------------------------------------------------
 // Source-side reachability (canonical cut) after the maximum preflow:
 // closure of {v : e(v) > 0} over residual edges.
-__device__ void reach_init_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0, int32_t* cnt0) {
-  const int64_t g = (int64_t)t * TV + threadIdx.x;
+__device__ void reach_init_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id0, int32_t* list0,
+                                int32_t* cnt0) {
+  const int l = threadIdx.x;
+  const int64_t g = (int64_t)t * TV + l;
   const bool seed = __ldcg(P.e + g) > 0;
   P.reach[g] = seed ? 1 : 0;
-  const int any = __syncthreads_or(seed);
-  if (threadIdx.x == 0 && any) {
-    P.stamp_bfs[t] = id0;
-    list0[atomicAdd(cnt0, 1)] = t;
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+  if (seed) {
+    const int fb = face_bits(l & 7, (l >> 3) & 7, l >> 6);
+    atomicOr(&S.flags, fb | 64);
   }
+  __syncthreads();
+  const int fl = S.flags;
+  if (l == 0 && (fl & 64)) queue_tile(P, P.stamp_bfs, t, id0, list0, cnt0);
+  if (l < 6 && ((fl >> l) & 1)) {
+    const int nt = __ldcg(P.nbr + l * P.T + t);
+    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id0, list0, cnt0);
+  }
+  __syncthreads();
 }
 
 __device__ void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
@@ -376,7 +405,7 @@ __device__ void reach_tile(const DevPool& P, const int t, ReachShared& S, const 
   __syncthreads();
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0 && atomicExch(P.stamp_bfs + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
+    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id_next, list_next, cnt_next);
   }
   __syncthreads();
 }

@@ -166,3 +166,40 @@ def test_resolve_after_reupload_is_identical():
     assert res[0] == res[1] == res[2]
     f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
     assert res[0][0] == f0
+
+
+def _face_case(X=16, Y=8, Z=8, sink_x=7, src_x=12, nlink=5):
+    """Sink capacity only on the +x face of the first tile, source capacity only
+    inside the second tile: the BFS seeds sit on a tile face and the second
+    tile has none of its own."""
+    N = X * Y * Z
+    capS = np.zeros((Z, Y, X), np.int32)
+    capT = np.zeros((Z, Y, X), np.int32)
+    capT[:, :, sink_x] = 3
+    capS[:, :, src_x] = 7
+    fx = np.full((Z, Y, X), nlink, np.int32)
+    fx[:, :, -1] = 0
+    z = np.zeros(N, np.int32)
+    return X, Y, Z, capS.reshape(-1), capT.reshape(-1), [fx.reshape(-1), z, z]
+
+
+@pytest.mark.parametrize("policy", ["default", "host_loop"])
+@pytest.mark.parametrize("sink_x,src_x", [(7, 12), (8, 3), (7, 8), (0, 15)])
+def test_seeds_on_tile_faces(sink_x, src_x, policy):
+    X, Y, Z, capS, capT, fwd = _face_case(sink_x=sink_x, src_x=src_x)
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd)
+    flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, None, POLICIES[policy])
+    assert f0 > 0
+    assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
+
+
+@pytest.mark.parametrize("policy", ["default", "host_loop"])
+@pytest.mark.parametrize("seed", range(8))
+def test_sparse_terminals_match_oracle(seed, policy):
+    """Very few t-links on a well connected grid: seeds land on tile faces and
+    many tiles have none (exercises BFS and reachability across tiles)."""
+    X, Y, Z = 40, 24, 17
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, 500 + seed, zero_frac=0.995, nmax=30)
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, bwd, POLICIES[policy])
+    assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
