@@ -35,14 +35,15 @@ class CgcError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("struct_size", C.c_int32), ("local_pulses", C.c_int32), ("sweeps_per_relabel", C.c_int32),
                 ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
-                ("reserved", C.c_int32 * 10)]
+                ("region_relabels", C.c_int32), ("reserved", C.c_int32 * 9)]
 
 
 class Stats(C.Structure):
     _fields_ = [("flow", C.c_int64), ("sweeps", C.c_int64), ("global_relabels", C.c_int64),
                 ("bfs_rounds", C.c_int64), ("tiles_swept", C.c_int64), ("tiles_relabelled", C.c_int64),
                 ("pulses", C.c_int64), ("solve_ms", C.c_double), ("kernel_ms", C.c_double),
-                ("launches", C.c_int64), ("reserved", C.c_int64 * 6)]
+                ("launches", C.c_int64), ("bfs_ms", C.c_double), ("sweep_ms", C.c_double),
+                ("reach_ms", C.c_double), ("reserved", C.c_int64 * 3)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -120,7 +121,7 @@ def check(rc: int) -> None:
 
 
 def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
-            persistent: int = 0) -> Options:
+            persistent: int = 0, region_relabels: int = 0) -> Options:
     o = Options()
     o.struct_size = C.sizeof(Options)
     o.local_pulses = local_pulses
@@ -128,4 +129,5 @@ def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 
     o.schedule = schedule
     o.max_sweeps = max_sweeps
     o.persistent = persistent
+    o.region_relabels = region_relabels
     return o

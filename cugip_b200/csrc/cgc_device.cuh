@@ -40,7 +40,13 @@ enum Counter {
 };
 
 // statistics in DevPool::stats (unsigned long long)
-enum Stat { S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5, S_NSTATS = 8 };
+enum Stat {
+  S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5,
+  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_NSTATS = 12
+};
+
+// BFS seed summary of a tile (DevPool::tflag)
+enum TileFlag { TF_ALL_SEED = 1, TF_FACE0 = 2 /* bits 1..6: a seed on face d */, TF_HAS_SEED = 128 };
 
 struct InstGeo {
   int32_t X, Y, Z;      // voxel extents
@@ -63,6 +69,7 @@ struct DevPool {
   const int32_t* tinst; // T: instance of the tile
   const uint8_t* tpar;  // T: (tx+ty+tz)&1
   uint8_t* act;         // T: tile holds an active voxel (e>0, h<INF)
+  uint8_t* tflag;       // T: BFS seed summary (TF_* bits)
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
   uint32_t* stamp_sw;   // T: last sweep the tile was queued for
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   const int mcap = min(s, c);
   const int e = s - mcap, rT = c - mcap;
   long long inflow = e;
-  unsigned m = rT > 0 ? 64u : 0u;
+  unsigned m = (rT > 0 ? 64u : 0u) | (e > 0 ? 128u : 0u);
   bool bad = false;
 #pragma unroll
   for (int d = 0; d < 6; ++d) {
@@ -155,10 +155,10 @@ __global__ void k_zero_axis(DevPool P, int inst, int axis) {
 }
 
 // Host-driven schedule: one launch per sweep / BFS round.
-__global__ void __launch_bounds__(512, 2) k_sweep_list(DevPool P, const int32_t* list, const int32_t* cnt, int L) {
+__global__ void __launch_bounds__(512, 2) k_sweep_list(DevPool P, const int32_t* list, const int32_t* cnt, int L, int R) {
   __shared__ SweepShared S;
   const int n = *cnt;
-  for (int i = blockIdx.x; i < n; i += gridDim.x) sweep_tile<false>(P, list[i], L, S, 0, nullptr, nullptr, 0, nullptr, nullptr);
+  for (int i = blockIdx.x; i < n; i += gridDim.x) sweep_tile<false>(P, list[i], L, R, S, 0, nullptr, nullptr, 0, nullptr, nullptr);
 }
 
 __global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
@@ -167,9 +167,13 @@ __global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
   warp_append(pred, t, list, cnt);
 }
 
-__global__ void __launch_bounds__(512) k_bfs_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
+__global__ void __launch_bounds__(512) k_bfs_init(DevPool P) {
   __shared__ BfsShared S;
-  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, S, id0, list0, cnt0);
+  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, S);
+}
+
+__global__ void k_bfs_queue(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  bfs_queue_tile(P, blockIdx.x * blockDim.x + threadIdx.x, id0, list0, cnt0);
 }
 
 __global__ void __launch_bounds__(512, 2) k_bfs_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
@@ -222,7 +226,8 @@ __device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
 __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }
 
 struct SolveParams {
-  int L;                 // pulses per tile visit
+  int L;                 // pulses per tile visit (per region-relabel round)
+  int R;                 // region-relabel rounds per tile visit (0: pulses only)
   int K;                 // sweep pairs between global relabels
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
@@ -246,6 +251,13 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   int64_t s = 0;        // sweep index; sweep s uses list s&3 and stamp id s+1
   int64_t sweeps = 0;
   long long rounds = 0, relabels = 0;
+  unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0;
+  uint64_t tmark = globaltimer_ns();
+  auto lap = [&](unsigned long long& acc) {
+    const uint64_t now = globaltimer_ns();
+    acc += now - tmark;
+    tmark = now;
+  };
   for (;;) {
     // ------------------------------------------------ exact global relabel
     if (b == 0 && tid == 0) {
@@ -253,7 +265,9 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
       sc[0] = sc[1] = sc[2] = sc[3] = 0;
     }
     if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs, bfs_id, bl[0], bc + 0);
+    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x) bfs_queue_tile(P, t0 + tid, bfs_id, bl[0], bc + 0);
     if (!grid_sync(P, prm.limit_ns)) return;
     int k = 0;
     for (;;) {
@@ -267,6 +281,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     bfs_id += k + 1;
     rounds += k;
     ++relabels;
+    lap(ns_bfs);
     // ------------------------------------------------ active tiles -> parity lists
     s += 2;  // fresh stamp ids for the lists built here
     for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
@@ -289,12 +304,14 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
       if (n == 0 && ld_cnt(sc + ((s + 1) & 3)) == 0) break;
       if (b == 0 && tid == 0) sc[(s + 3) & 3] = 0;
       for (int i = b; i < n; i += G)
-        sweep_tile<true>(P, __ldcg(sl[s & 3] + i), prm.L, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+        sweep_tile<true>(P, __ldcg(sl[s & 3] + i), prm.L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
                          (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3));
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
     }
+    lap(ns_sweep);
   }
+  lap(ns_bfs);
   // ------------------------------------------------ source-side reachability
   if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
   if (!grid_sync(P, prm.limit_ns)) return;
@@ -313,6 +330,10 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     P.stats[S_SWEEPS] = (unsigned long long)sweeps;
     P.stats[S_RELABELS] = (unsigned long long)relabels;
     P.stats[S_ROUNDS] = (unsigned long long)rounds;
+    lap(ns_reach);
+    P.stats[S_NS_BFS] = ns_bfs;
+    P.stats[S_NS_SWEEP] = ns_sweep;
+    P.stats[S_NS_REACH] = ns_reach;
   }
 }
 
@@ -426,6 +447,7 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   const int64_t o_ti = off; off += al(T * 4);
   const int64_t o_tp = off; off += al(T);
   const int64_t o_act = off; off += al(T);
+  const int64_t o_tf = off; off += al(T);
   const int64_t o_sb = off; off += al(T * 4);
   const int64_t o_ss = off; off += al(T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
@@ -443,7 +465,7 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   d.e = (int32_t*)(base + o_e); d.h = (int32_t*)(base + o_h); d.rT = (int32_t*)(base + o_rT);
   d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
   d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
-  d.act = (uint8_t*)(base + o_act); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
+  d.act = (uint8_t*)(base + o_act); d.tflag = (uint8_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
   d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
   d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
   d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
@@ -537,12 +559,14 @@ static cgc_options resolve_options(const cgc_options* o) {
   r.schedule = CGC_SCHED_PARITY;
   r.max_sweeps = 1 << 20;
   r.persistent = 1;
+  r.region_relabels = 1;
   if (o) {
     if (o->local_pulses > 0) r.local_pulses = std::min(o->local_pulses, 64);
     if (o->sweeps_per_relabel > 0) r.sweeps_per_relabel = o->sweeps_per_relabel;
     if (o->schedule) r.schedule = o->schedule;
     if (o->max_sweeps > 0) r.max_sweeps = o->max_sweeps;
     if (o->persistent) r.persistent = o->persistent;
+    if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
   }
   return r;
 }
@@ -555,7 +579,10 @@ static int host_bfs(Pool& p, uint32_t& id, int64_t& rounds) {
   CGC_CUDA(cudaMemsetAsync(d.cnt + C_BFS0, 0, 3 * 4, p.stream));
   const int gi = std::min<int>(d.T, p.sms * 8);
   if (REACH) { k_reach_init<<<gi, 512, 0, p.stream>>>(d, id, bl[0], d.cnt + C_BFS0); note_launch(); }
-  else { k_bfs_init<<<gi, 512, 0, p.stream>>>(d, id, bl[0], d.cnt + C_BFS0); note_launch(); }
+  else {
+    k_bfs_init<<<gi, 512, 0, p.stream>>>(d); note_launch();
+    k_bfs_queue<<<(d.T + 255) / 256, 256, 0, p.stream>>>(d, id, bl[0], d.cnt + C_BFS0); note_launch();
+  }
   CGC_CUDA(cudaGetLastError());
   for (int k = 0;; ++k) {
     CGC_CUDA(cudaMemcpyAsync(p.pinned_cnt, d.cnt + C_BFS0 + k % 3, 4, cudaMemcpyDeviceToHost, p.stream));
@@ -606,6 +633,7 @@ static int pool_solve(Pool& p, const cgc_options* opts) {
   if (o.persistent > 0) {
     SolveParams prm;
     prm.L = o.local_pulses;
+    prm.R = o.region_relabels;
     prm.K = o.sweeps_per_relabel;
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
@@ -635,7 +663,7 @@ static int pool_solve(Pool& p, const cgc_options* opts) {
           CGC_CUDA(cudaMemsetAsync(d.cnt + C_SW0 + par, 0, 4, p.stream));
           k_compact<<<(d.T + 255) / 256, 256, 0, p.stream>>>(d, par, sl + par * d.T, d.cnt + C_SW0 + par); note_launch();
         }
-        k_sweep_list<<<p.sweep_blocks, 512, 0, p.stream>>>(d, sl + par * d.T, d.cnt + C_SW0 + par, o.local_pulses); note_launch();
+        k_sweep_list<<<p.sweep_blocks, 512, 0, p.stream>>>(d, sl + par * d.T, d.cnt + C_SW0 + par, o.local_pulses, o.region_relabels); note_launch();
         CGC_CUDA(cudaGetLastError());
         ++sweeps;
       }
@@ -675,6 +703,9 @@ static int pool_solve(Pool& p, const cgc_options* opts) {
   p.st.solve_ms = ms;
   p.st.kernel_ms = kms;
   p.st.launches = g_launches.load() - launches0;
+  p.st.bfs_ms = 1e-6 * (double)stats[S_NS_BFS];
+  p.st.sweep_ms = 1e-6 * (double)stats[S_NS_SWEEP];
+  p.st.reach_ms = 1e-6 * (double)stats[S_NS_REACH];
   for (auto& u : p.uploaded) u = 0;
   p.solved = true;
   return ok();

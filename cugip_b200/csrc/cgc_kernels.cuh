@@ -84,10 +84,12 @@ __device__ __forceinline__ void for_halo_entry(int l, F&& fn) {
   }
 }
 
-__device__ __forceinline__ void load_halo_heights(const DevPool& P, int t, int* sh) {
+__device__ __forceinline__ void load_halo_heights(const DevPool& P, int t, int (*sh)[HALO]) {
   for_halo_entry(threadIdx.x, [&](int f, int hi, int src) {
     const int nt = __ldcg(P.nbr + f * P.T + t);
-    sh[hi] = (nt >= 0) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
+    const int v = (nt >= 0) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
+    sh[0][hi] = v;
+    sh[1][hi] = v;
   });
 }
 
@@ -119,21 +121,23 @@ __device__ __forceinline__ long long block_sum64(long long v, long long* red) {
   return s;
 }
 
+// Shared state is double buffered (pulse / iteration parity), so one
+// pulse needs two barriers and one BFS iteration needs one.
 struct SweepShared {
-  int h[HALO];
-  int out[6][TV];
+  int h[2][HALO];
+  int out[2][6][TV];
   long long red[16];
   int flags;
 };
 
 struct BfsShared {
-  int h[HALO];
+  int h[2][HALO];
   long long red[16];
   int flags;
 };
 
 struct ReachShared {
-  unsigned char rc[HALO];
+  unsigned char rc[2][HALO];
   unsigned char m[HALO];
   long long red[16];
   int flags;
@@ -145,7 +149,7 @@ struct ReachShared {
 //   tiles it pushed into for sweep id_next (persistent schedule); otherwise
 //   only the act[] flags are maintained (host-driven schedule).
 template <bool APPEND>
-__device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShared& S,
+__device__ void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self) {
   const int l = threadIdx.x;
@@ -157,7 +161,7 @@ __device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShar
 #pragma unroll
   for (int d = 0; d < 6; ++d) r[d] = __ldcg(P.r + d * Np + g);
   const int hi = halo_index(x, y, z);
-  S.h[hi] = h;
+  S.h[0][hi] = h;
   load_halo_heights(P, t, S.h);
   const int inst = __ldcg(P.tinst + t);
   const int hdead = P.geo[inst].hdead;
@@ -167,61 +171,92 @@ __device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShar
   int acc[6] = {0, 0, 0, 0, 0, 0};  // flow pushed out of the tile, per face
   int sink = 0;
   int pulses = 0;
-  for (int p = 0; p < L; ++p) {
-    int hn[6];
+  int cur = 0;
+  for (int round = 0;; ++round) {
+    if (R > 0) {
+      // Region relabel: exact distance d(v) to the sink or to the (frozen)
+      // halo inside the tile, then h = max(h, d).  d is a lower bound of the
+      // true distance and max(h, d) keeps every residual edge valid, so this
+      // is an ordinary (multi-step) relabel; d = INF means v cannot reach the
+      // sink at all.
+      int dd = (rT > 0) ? 1 : INF;
+      S.h[cur][hi] = dd;
+      __syncthreads();
+      for (int it = 0; it < 600; ++it) {  // Bellman-Ford: < 512 steps in a tile
+        int mn = dd;
 #pragma unroll
-    for (int d = 0; d < 6; ++d) hn[d] = S.h[hi + hoff(d)];
-    int pushed[6] = {0, 0, 0, 0, 0, 0};
-    if (e > 0 && h < INF) {
-      if (rT > 0 && h == 1) {
-        const int dl = min(e, rT);
-        e -= dl; rT -= dl; sink += dl;
+        for (int d = 0; d < 6; ++d)
+          if (r[d] > 0) mn = min(mn, S.h[cur][hi + hoff(d)] + 1);
+        S.h[cur ^ 1][hi] = mn;
+        const int any = __syncthreads_or(mn < dd);
+        dd = mn;
+        cur ^= 1;
+        if (!any) break;
       }
+      int hn = max(h, dd);
+      if (hn >= hdead) hn = INF;
+      h = hn;
+      S.h[cur][hi] = h;
+      __syncthreads();
+    }
+    int any = 1;
+    for (int p = 0; p < L; ++p) {
+      int hn[6];
 #pragma unroll
-      for (int d = 0; d < 6; ++d) {
-        if (e > 0 && r[d] > 0 && hn[d] == h - 1) {
-          const int dl = min(e, r[d]);
-          e -= dl; r[d] -= dl; pushed[d] = dl;
+      for (int d = 0; d < 6; ++d) hn[d] = S.h[cur][hi + hoff(d)];
+      int pushed[6] = {0, 0, 0, 0, 0, 0};
+      if (e > 0 && h < INF) {
+        if (rT > 0 && h == 1) {
+          const int dl = min(e, rT);
+          e -= dl; rT -= dl; sink += dl;
+        }
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+          if (e > 0 && r[d] > 0 && hn[d] == h - 1) {
+            const int dl = min(e, r[d]);
+            e -= dl; r[d] -= dl; pushed[d] = dl;
+          }
         }
       }
-    }
-#pragma unroll
-    for (int d = 0; d < 6; ++d) {
-      if (inside(d, x, y, z)) S.out[d][l] = pushed[d];
-      else acc[d] += pushed[d];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int d = 0; d < 6; ++d) {
-      if (inside(d, x, y, z)) {
-        const int din = S.out[d ^ 1][l + loff(d)];
-        e += din; r[d] += din;
-      }
-    }
-    int hnew = h;
-    if (e > 0 && h < INF) {
-      bool adm = (rT > 0 && h == 1);
-      int mn = (rT > 0) ? 0 : INF;
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
-        if (r[d] > 0) { adm = adm || (hn[d] == h - 1); mn = min(mn, hn[d]); }
+        if (inside(d, x, y, z)) S.out[cur][d][l] = pushed[d];
+        else acc[d] += pushed[d];
       }
-      if (!adm) {
-        hnew = (mn >= INF) ? INF : mn + 1;
-        if (hnew >= hdead) hnew = INF;
+      __syncthreads();
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (inside(d, x, y, z)) {
+          const int din = S.out[cur][d ^ 1][l + loff(d)];
+          e += din; r[d] += din;
+        }
       }
+      int hnew = h;
+      if (e > 0 && h < INF) {
+        bool adm = (rT > 0 && h == 1);
+        int mn = (rT > 0) ? 0 : INF;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+          if (r[d] > 0) { adm = adm || (hn[d] == h - 1); mn = min(mn, hn[d]); }
+        }
+        if (!adm) {
+          hnew = (mn >= INF) ? INF : mn + 1;
+          if (hnew >= hdead) hnew = INF;
+        }
+      }
+      ++pulses;
+      S.h[cur ^ 1][hi] = hnew;
+      any = __syncthreads_or(e > 0 && hnew < INF);
+      h = hnew;
+      cur ^= 1;
+      if (!any) break;
     }
-    ++pulses;
-    const int any = __syncthreads_or(e > 0 && hnew < INF);
-    h = hnew;
-    S.h[hi] = h;
-    if (!any) break;
-    __syncthreads();
+    if (!any || round + 1 >= max(R, 1)) break;
   }
 
   // write back the tile
   P.e[g] = e; P.h[g] = h; P.rT[g] = rT;
-  unsigned m = (rT > 0) ? 64u : 0u;
+  unsigned m = ((rT > 0) ? 64u : 0u) | ((e > 0) ? 128u : 0u);
 #pragma unroll
   for (int d = 0; d < 6; ++d) { P.r[d * Np + g] = r[d]; m |= (r[d] > 0 ? 1u : 0u) << d; }
   P.rmask[g] = (uint8_t)m;
@@ -234,7 +269,7 @@ __device__ void sweep_tile(const DevPool& P, const int t, const int L, SweepShar
       const int64_t ng = (int64_t)nt * TV + l + xoff(d);
       atomicAdd(P.e + ng, acc[d]);
       atomicAdd(P.r + (d ^ 1) * Np + ng, acc[d]);
-      atomicOr((unsigned*)(P.rmask + (ng & ~(int64_t)3)), 1u << (8 * (int)(ng & 3) + (d ^ 1)));
+      atomicOr((unsigned*)(P.rmask + (ng & ~(int64_t)3)), (128u | (1u << (d ^ 1))) << (8 * (int)(ng & 3)));
       atomicOr(&S.flags, 1 << d);
     }
   }
@@ -268,29 +303,44 @@ __device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, in
   if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
 }
 
-__device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id0, int32_t* list0,
-                              int32_t* cnt0) {
+__device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
-  const bool seed = (__ldcg(P.rmask + g) & 64u) != 0;
+  const unsigned rm = __ldcg(P.rmask + g);
+  const bool seed = (rm & 64u) != 0;
   P.h[g] = seed ? 1 : INF;
   if (l == 0) S.flags = 0;
   __syncthreads();
-  if (seed) {
-    const int fb = face_bits(l & 7, (l >> 3) & 7, l >> 6);
-    atomicOr(&S.flags, fb | 64);
-  }
-  __syncthreads();
-  const int fl = S.flags;
+  if (seed) atomicOr(&S.flags, (face_bits(l & 7, (l >> 3) & 7, l >> 6) << 1) | TF_HAS_SEED);
+  const int all_seed = __syncthreads_and(seed);
+  // a tile whose voxels are all seeds is final at h = 1 and is never visited
+  int act = 0;
+  if (all_seed) act = __syncthreads_or((rm & 128u) != 0);
   if (l == 0) {
-    P.act[t] = 0;
-    if (fl & 64) queue_tile(P, P.stamp_bfs, t, id0, list0, cnt0);
-  }
-  if (l < 6 && ((fl >> l) & 1)) {
-    const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id0, list0, cnt0);
+    P.tflag[t] = (uint8_t)(S.flags | (all_seed ? TF_ALL_SEED : 0));
+    P.act[t] = (uint8_t)(act ? 1 : 0);
   }
   __syncthreads();
+}
+
+// Second BFS seeding step, one thread per tile: queue every tile that is not
+// all seeds and holds a seed or touches a seed on a neighbour's face.
+__device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0,
+                                               int32_t* cnt0) {
+  bool q = false;
+  if (t < P.T) {
+    const int f = __ldcg(P.tflag + t);
+    if (!(f & TF_ALL_SEED)) {
+      q = (f & TF_HAS_SEED) != 0;
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        const int nt = __ldcg(P.nbr + d * P.T + t);
+        if (nt >= 0 && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1)) q = true;
+      }
+    }
+    if (q) P.stamp_bfs[t] = id0;
+  }
+  warp_append(q, t, list0, cnt0);
 }
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
@@ -303,29 +353,30 @@ __device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint
   int h = __ldcg(P.h + g);
   const int h0 = h;
   const unsigned m = __ldcg(P.rmask + g);
-  const int e = __ldcg(P.e + g);
+  const bool has_excess = (m & 128u) != 0;
   const int hi = halo_index(x, y, z);
-  S.h[hi] = h;
+  S.h[0][hi] = h;
   load_halo_heights(P, t, S.h);
   if (l == 0) S.flags = 0;
   __syncthreads();
+  int cur = 0;
   for (int it = 0; it < 1024; ++it) {  // converges in < 512 steps (path length in a tile)
     int mn = h;
 #pragma unroll
     for (int d = 0; d < 6; ++d)
-      if ((m >> d) & 1u) mn = min(mn, S.h[hi + hoff(d)] + 1);
-    const bool ch = mn < h;
-    const int any = __syncthreads_or(ch);
+      if ((m >> d) & 1u) mn = min(mn, S.h[cur][hi + hoff(d)] + 1);
+    S.h[cur ^ 1][hi] = mn;
+    const int any = __syncthreads_or(mn < h);
+    h = mn;
+    cur ^= 1;
     if (!any) break;
-    if (ch) { h = mn; S.h[hi] = h; }
-    __syncthreads();
   }
   if (h < h0) {
     P.h[g] = h;
     const int fb = face_bits(x, y, z);
     if (fb) atomicOr(&S.flags, fb);
   }
-  const int act = __syncthreads_or(e > 0 && h < INF);
+  const int act = __syncthreads_or(has_excess && h < INF);
   if (l == 0) {
     P.act[t] = (uint8_t)(act ? 1 : 0);
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
@@ -344,7 +395,7 @@ __device__ void reach_init_tile(const DevPool& P, const int t, ReachShared& S, c
                                 int32_t* cnt0) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
-  const bool seed = __ldcg(P.e + g) > 0;
+  const bool seed = (__ldcg(P.rmask + g) & 128u) != 0;
   P.reach[g] = seed ? 1 : 0;
   if (l == 0) S.flags = 0;
   __syncthreads();
@@ -370,32 +421,34 @@ __device__ void reach_tile(const DevPool& P, const int t, ReachShared& S, const 
   int rc = __ldcg(P.reach + g);
   const int rc0 = rc;
   const int hi = halo_index(x, y, z);
-  S.rc[hi] = (unsigned char)rc;
+  S.rc[0][hi] = (unsigned char)rc;
   S.m[hi] = __ldcg(P.rmask + g);
   for_halo_entry(l, [&](int f, int hh, int src) {
     const int nt = __ldcg(P.nbr + f * P.T + t);
+    unsigned char rv = 0, mv = 0;
     if (nt >= 0) {
-      S.rc[hh] = __ldcg(P.reach + (int64_t)nt * TV + src);
-      S.m[hh] = __ldcg(P.rmask + (int64_t)nt * TV + src);
-    } else {
-      S.rc[hh] = 0; S.m[hh] = 0;
+      rv = __ldcg(P.reach + (int64_t)nt * TV + src);
+      mv = __ldcg(P.rmask + (int64_t)nt * TV + src);
     }
+    S.rc[0][hh] = rv; S.rc[1][hh] = rv; S.m[hh] = mv;
   });
   if (l == 0) S.flags = 0;
   __syncthreads();
+  int cur = 0;
   for (int it = 0; it < 1024; ++it) {
     bool ch = false;
     if (!rc) {
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         const int u = hi + hoff(d);
-        if (S.rc[u] && ((S.m[u] >> (d ^ 1)) & 1u)) ch = true;
+        if (S.rc[cur][u] && ((S.m[u] >> (d ^ 1)) & 1u)) ch = true;
       }
     }
+    if (ch) rc = 1;
+    S.rc[cur ^ 1][hi] = (unsigned char)rc;
     const int any = __syncthreads_or(ch);
+    cur ^= 1;
     if (!any) break;
-    if (ch) { rc = 1; S.rc[hi] = 1; }
-    __syncthreads();
   }
   if (rc && !rc0) {
     P.reach[g] = 1;

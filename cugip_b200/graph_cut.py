@@ -55,7 +55,8 @@ class Policy:
     """Runtime counterpart of GraphCutPolicy (detail/graph_cut_policies.hpp:23-89)."""
 
     def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0,
-                 max_sweeps: int = 0, persistent: int = 0):
+                 max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0):
+        self.region_relabels = region_relabels
         self.local_pulses = local_pulses
         self.sweeps_per_relabel = sweeps_per_relabel
         self.schedule = schedule
@@ -64,7 +65,7 @@ class Policy:
 
     def options(self) -> _lib.Options:
         return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
-                            self.persistent)
+                            self.persistent, self.region_relabels)
 
 
 class GridGraph:

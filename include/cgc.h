@@ -75,7 +75,8 @@ typedef struct cgc_options {
   int32_t schedule;           /* CGC_SCHED_* (default parity) */
   int32_t max_sweeps;         /* safety cap on sweep pairs, default 1<<20 */
   int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
-  int32_t reserved[10];
+  int32_t region_relabels;    /* region-relabel rounds per tile visit (default 1, -1 = none) */
+  int32_t reserved[9];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */
@@ -90,7 +91,10 @@ typedef struct cgc_stats {
   double  solve_ms;          /* device time of the last maxflow (preparation + solve) */
   double  kernel_ms;         /* device time of the solve kernel(s) alone */
   int64_t launches;          /* kernels launched by the last maxflow */
-  int64_t reserved[6];
+  double  bfs_ms;            /* persistent solve: time in exact global relabels */
+  double  sweep_ms;          /* persistent solve: time in push sweeps */
+  double  reach_ms;          /* persistent solve: time in the source-side reachability */
+  int64_t reserved[3];
 } cgc_stats;
 
 /* Kernels launched by this library on the calling process since load

@@ -24,6 +24,9 @@ POLICIES = {
     "L4_K2": Policy(local_pulses=4, sweeps_per_relabel=2),
     "L32_K32": Policy(local_pulses=32, sweeps_per_relabel=32),
     "host_L2": Policy(local_pulses=2, sweeps_per_relabel=3, persistent=-1),
+    "no_region": Policy(region_relabels=-1),
+    "R3_L2": Policy(local_pulses=2, region_relabels=3, sweeps_per_relabel=2),
+    "host_R2": Policy(region_relabels=2, persistent=-1),
 }
 
 
