@@ -1,0 +1,245 @@
+// cgc/graph_cut.hpp — header-only C++ facade over the C ABI of libcgc.so that
+// mirrors cugip's graph-cut API, so reference callers switch by changing the
+// include and the namespace:
+//
+//   cugip::Graph<TFlow>            include/cugip/advanced_operations/graph_cut.hpp:47-146
+//   cugip::EdgeRecord              include/cugip/advanced_operations/detail/edge_record.hpp:10-29
+//   cugip::DummyTraceObject        include/cugip/advanced_operations/graph_cut.hpp:26-45
+//   cugip::GraphCutPolicy          include/cugip/advanced_operations/detail/graph_cut_policies.hpp:80-89
+//   CUGIP_CHECK_RESULT -> throw    include/cugip/exception.hpp:33-47
+//
+// Capacities are exact integers: TFlow may be an integer type or a floating
+// type holding integral values in [0, 2^31); anything else throws.  The flow is
+// returned as TFlow (computed in int64).
+#pragma once
+
+#include <cstdint>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../cgc.h"
+
+namespace cgc {
+
+class Exception : public std::runtime_error {
+ public:
+  Exception(int code, const std::string& what) : std::runtime_error(what), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+inline void check(int rc, const char* where) {
+  if (rc != CGC_OK) throw Exception(rc, std::string(where) + ": " + cgc_last_error());
+}
+
+// Same layout as cugip::EdgeRecord: a union of a 64-bit id with
+// {second, first}; the constructor stores (min, max).
+typedef unsigned NodeId;
+struct EdgeRecord {
+  EdgeRecord(NodeId a, NodeId b) : second(a < b ? b : a), first(a < b ? a : b) {}
+  EdgeRecord() : second(0), first(0) {}
+  NodeId second;
+  NodeId first;
+};
+static_assert(sizeof(EdgeRecord) == 8, "EdgeRecord layout");
+
+// Runtime policy (the reference's compile-time GraphCutPolicy knobs).
+struct GraphCutPolicy {
+  int local_pulses = 0;        // pulses per region-relabel round of a tile visit
+  int region_relabels = 0;     // region relabels per tile visit (-1: none)
+  int sweeps_per_relabel = 0;  // sweep pairs between exact global relabels
+  int persistent = 0;          // 1: one cooperative launch, -1: host loop
+  cgc_options options() const {
+    cgc_options o{};
+    o.struct_size = sizeof(cgc_options);
+    o.local_pulses = local_pulses;
+    o.region_relabels = region_relabels;
+    o.sweeps_per_relabel = sweeps_per_relabel;
+    o.persistent = persistent;
+    return o;
+  }
+};
+
+// Trace protocol of the reference.  The solve runs as one device launch, so
+// the per-iteration hooks are replayed after it with the solve statistics
+// (one iteration per exact global relabel).
+struct DummyTraceObject {
+  void computationStarted(const cgc_stats&) {}
+  void beginIteration(int) {}
+  void afterRelabel(int, const std::vector<int>&) {}
+  void afterPush(int, bool, const cgc_stats&) {}
+  template <typename TFlow>
+  void computationFinished(TFlow, const cgc_stats&) {}
+};
+
+namespace detail {
+template <typename T>
+std::vector<int32_t> to_i32(const T* a, size_t n, const char* what) {
+  std::vector<int32_t> out(n);
+  for (size_t i = 0; i < n; ++i) {
+    const double v = static_cast<double>(a[i]);
+    if (!(v >= 0.0) || v > 2147483647.0 || (std::is_floating_point<T>::value && std::floor(v) != v))
+      throw Exception(CGC_ERR_ARG, std::string(what) + ": capacities must be integers in [0, 2^31)");
+    out[i] = static_cast<int32_t>(v);
+  }
+  return out;
+}
+}  // namespace detail
+
+// X*Y*Z grid graph with per-axis n-link volumes (vertex id = x + X*(y + Y*z)).
+class GridGraph {
+ public:
+  GridGraph(int X, int Y, int Z, void* stream = nullptr) : X_(X), Y_(Y), Z_(Z) {
+    check(cgc_grid_create(X, Y, Z, stream, &g_), "cgc_grid_create");
+  }
+  explicit GridGraph(cgc_grid* adopt, int X, int Y, int Z) : g_(adopt), X_(X), Y_(Y), Z_(Z) {}
+  GridGraph(const GridGraph&) = delete;
+  GridGraph& operator=(const GridGraph&) = delete;
+  ~GridGraph() { cgc_grid_destroy(g_); }
+
+  size_t size() const { return (size_t)X_ * Y_ * Z_; }
+  void set_tweights(const int32_t* capS, const int32_t* capT) { check(cgc_grid_set_tlinks(g_, capS, capT), "set_tweights"); }
+  void set_nweights(int axis, const int32_t* fwd, const int32_t* bwd) {
+    check(cgc_grid_set_nlinks(g_, axis, fwd, bwd), "set_nweights");
+  }
+  int64_t max_flow(const GraphCutPolicy* policy = nullptr) {
+    int64_t f = 0;
+    cgc_options o;
+    if (policy) o = policy->options();
+    check(cgc_grid_maxflow(g_, policy ? &o : nullptr, &f), "max_flow");
+    return f;
+  }
+  void segments(int which, uint8_t* out, uint8_t mask = 255, uint8_t bg = 0) const {
+    check(cgc_grid_get_segments(g_, which, out, mask, bg), "fill_segments");
+  }
+  cgc_stats stats() const {
+    cgc_stats s;
+    check(cgc_grid_stats(g_, &s), "stats");
+    return s;
+  }
+  cgc_grid* handle() const { return g_; }
+
+ private:
+  cgc_grid* g_ = nullptr;
+  int X_, Y_, Z_;
+};
+
+// Drop-in for cugip::Graph<TFlow> (graph_cut.hpp:47-146).  The edge list must
+// form a 6-connected grid with linear vertex ids; other graphs throw
+// Exception(CGC_ERR_NOT_GRID).  Unlike the reference, the graph can be solved
+// again after setting new weights.
+template <typename TFlow>
+class Graph {
+ public:
+  typedef int VertexId;
+  typedef TFlow EdgeWeight;
+
+  void set_vertex_count(int count) {
+    n_ = count;
+    grid_.reset();
+  }
+
+  void set_nweights(int edge_count, const EdgeRecord* edges, const EdgeWeight* fwd, const EdgeWeight* bwd) {
+    std::vector<uint32_t> a(edge_count), b(edge_count);
+    for (int i = 0; i < edge_count; ++i) { a[i] = edges[i].first; b[i] = edges[i].second; }
+    std::vector<int32_t> f = detail::to_i32(fwd, edge_count, "set_nweights");
+    std::vector<int32_t> w = detail::to_i32(bwd, edge_count, "set_nweights");
+    cgc_grid* g = nullptr;
+    int32_t dims[3];
+    check(cgc_grid_create_from_edges(n_, edge_count, a.data(), b.data(), f.data(), w.data(), nullptr, &g, dims),
+          "set_nweights");
+    grid_.reset(new GridGraph(g, dims[0], dims[1], dims[2]));
+    if (!pending_s_.empty()) {
+      grid_->set_tweights(pending_s_.data(), pending_t_.data());
+      pending_s_.clear();
+      pending_t_.clear();
+    }
+  }
+
+  void set_tweights(const EdgeWeight* capSource, const EdgeWeight* capSink) {
+    std::vector<int32_t> s = detail::to_i32(capSource, (size_t)n_, "set_tweights");
+    std::vector<int32_t> t = detail::to_i32(capSink, (size_t)n_, "set_tweights");
+    if (!grid_) {  // the reference accepts t-links before n-links
+      pending_s_.swap(s);
+      pending_t_.swap(t);
+      return;
+    }
+    grid_->set_tweights(s.data(), t.data());
+  }
+
+  TFlow max_flow() {
+    DummyTraceObject trace;
+    return max_flow_with_tracing(trace);
+  }
+  template <typename TPolicy>
+  TFlow max_flow(TPolicy& policy) {
+    DummyTraceObject trace;
+    return max_flow_with_tracing(policy, trace);
+  }
+  template <typename TTraceObject>
+  TFlow max_flow_with_tracing(TTraceObject& trace) {
+    GraphCutPolicy policy;
+    return max_flow_with_tracing(policy, trace);
+  }
+  template <typename TPolicy, typename TTraceObject>
+  TFlow max_flow_with_tracing(TPolicy& policy, TTraceObject& trace) {
+    if (!grid_) throw Exception(CGC_ERR_STATE, "max_flow: set_nweights was not called");
+    cgc_stats before{};
+    trace.computationStarted(before);
+    const GraphCutPolicy& p = policy;
+    const int64_t f = grid_->max_flow(&p);
+    const cgc_stats st = grid_->stats();
+    const std::vector<int> no_levels;
+    for (int64_t i = 0; i < st.global_relabels; ++i) {
+      trace.beginIteration((int)i);
+      trace.afterRelabel((int)i, no_levels);
+      trace.afterPush((int)i, i + 1 == st.global_relabels, st);
+    }
+    trace.computationFinished(static_cast<TFlow>(f), st);
+    return static_cast<TFlow>(f);
+  }
+
+  // out[i] = mask for vertices that can reach the sink (cugip's fill_segments,
+  // graph_cut.hpp:304-333), background elsewhere.  out must be indexable by
+  // vertex id.
+  template <typename THostArrayView>
+  void fill_segments(THostArrayView out, uint8_t mask = 255, uint8_t background = 0) const {
+    fill(CGC_SEG_SINK_REACH, out, mask, background);
+  }
+  // The minimal source side of the minimum cut (the canonical cut).
+  template <typename THostArrayView>
+  void fill_source_segments(THostArrayView out, uint8_t mask = 255, uint8_t background = 0) const {
+    fill(CGC_SEG_SOURCE_MIN, out, mask, background);
+  }
+
+  GridGraph* grid() const { return grid_.get(); }
+
+ private:
+  template <typename THostArrayView>
+  void fill(int which, THostArrayView& out, uint8_t mask, uint8_t background) const {
+    if (!grid_) throw Exception(CGC_ERR_STATE, "fill_segments: no graph");
+    std::vector<uint8_t> tmp(grid_->size());
+    grid_->segments(which, tmp.data(), mask, background);
+    for (size_t i = 0; i < tmp.size(); ++i) out[i] = tmp[i];
+  }
+
+  struct GridPtr {
+    GridGraph* p = nullptr;
+    ~GridPtr() { delete p; }
+    void reset(GridGraph* q = nullptr) { delete p; p = q; }
+    GridGraph* get() const { return p; }
+    GridGraph* operator->() const { return p; }
+    explicit operator bool() const { return p != nullptr; }
+  };
+
+  int n_ = 0;
+  GridPtr grid_;
+  std::vector<int32_t> pending_s_, pending_t_;
+};
+
+}  // namespace cgc

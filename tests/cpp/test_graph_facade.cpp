@@ -1,0 +1,74 @@
+// Reference-style C++ use of the cgc facade: the 4x4 graph of the reference's
+// test/graph_cut.cu:13-67 through cgc::Graph<float> (the reference's float
+// API), the same through Graph<int>, and a grid through cgc::GridGraph.
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include <cgc/graph_cut.hpp>
+
+#define EXPECT(c)                                                       \
+  do {                                                                  \
+    if (!(c)) { std::printf("FAILED %s:%d %s\n", __FILE__, __LINE__, #c); std::exit(1); } \
+  } while (0)
+
+struct CountingTrace : cgc::DummyTraceObject {
+  int iterations = 0;
+  long long finished = -1;
+  void beginIteration(int) { ++iterations; }
+  template <typename T>
+  void computationFinished(T flow, const cgc_stats&) { finished = (long long)flow; }
+};
+
+template <typename W>
+void four_by_four() {
+  cgc::Graph<W> graph;
+  graph.set_vertex_count(16);
+  int v1[24] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11};
+  int v2[24] = {1, 2, 3, 5, 6, 7, 9, 10, 11, 13, 14, 15, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15};
+  cgc::EdgeRecord edges[24];
+  for (int i = 0; i < 24; ++i) edges[i] = cgc::EdgeRecord(v1[i], v2[i]);
+  W w[24] = {5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 1, 1, 1, 1, 5, 5, 5, 5};
+  W src[16] = {100, 100, 100, 100, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  W snk[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 100, 100, 100, 100};
+  graph.set_nweights(24, edges, w, w);
+  graph.set_tweights(src, snk);
+  CountingTrace trace;
+  W flow = graph.max_flow_with_tracing(trace);
+  EXPECT(flow == (W)4);
+  EXPECT(trace.finished == 4 && trace.iterations >= 1);
+  std::vector<unsigned char> seg(16);
+  graph.fill_segments(seg.data());
+  for (int i = 0; i < 16; ++i) EXPECT(seg[i] == (i < 8 ? 0 : 255));
+  graph.fill_source_segments(seg.data(), 1, 0);
+  for (int i = 0; i < 16; ++i) EXPECT(seg[i] == (i < 8 ? 1 : 0));
+  // solving again after re-setting the weights gives the same answer
+  graph.set_tweights(src, snk);
+  graph.set_nweights(24, edges, w, w);
+  EXPECT(graph.max_flow() == (W)4);
+}
+
+int main() {
+  four_by_four<float>();
+  four_by_four<int>();
+  // non-integral weights are rejected
+  bool threw = false;
+  try {
+    cgc::Graph<float> g;
+    g.set_vertex_count(2);
+    float s[2] = {0.5f, 0.f}, t[2] = {0.f, 1.f};
+    g.set_tweights(s, t);
+  } catch (const cgc::Exception& e) {
+    threw = e.code() == CGC_ERR_ARG;
+  }
+  EXPECT(threw);
+  // grid facade: a chain along x with a bottleneck
+  cgc::GridGraph g(16, 1, 1);
+  std::vector<int32_t> cs(16, 0), ct(16, 0), nx(16, 9), z(16, 0);
+  cs[0] = 50; ct[15] = 50; nx[7] = 3; nx[15] = 0;
+  g.set_tweights(cs.data(), ct.data());
+  g.set_nweights(CGC_AXIS_X, nx.data(), nx.data());
+  EXPECT(g.max_flow() == 3);
+  std::printf("cpp facade ok\n");
+  return 0;
+}

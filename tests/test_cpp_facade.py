@@ -1,0 +1,29 @@
+"""The C++ facade (include/cgc/graph_cut.hpp) used the way the reference's own
+test uses cugip::Graph (test/graph_cut.cu:13-67)."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "test_graph_facade.cpp")
+LIBDIR = os.path.join(ROOT, "cugip_b200")
+
+
+def compile_facade_test(tmp_path) -> str:
+    exe = str(tmp_path / "test_graph_facade")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    SRC, "-L", LIBDIR, "-lcgc", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+    return exe
+
+
+def test_facade_compiles_against_the_c_abi(tmp_path):
+    assert os.path.exists(compile_facade_test(tmp_path))
+
+
+@pytest.mark.gpu
+def test_facade_runs_reference_style_graph(tmp_path):
+    exe = compile_facade_test(tmp_path)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "cpp facade ok" in out.stdout
