@@ -142,6 +142,8 @@ class Graph {
   void set_vertex_count(int count) {
     n_ = count;
     grid_.reset();
+    tlink_s_.clear();
+    tlink_t_.clear();
   }
 
   void set_nweights(int edge_count, const EdgeRecord* edges, const EdgeWeight* fwd, const EdgeWeight* bwd) {
@@ -154,22 +156,15 @@ class Graph {
     check(cgc_grid_create_from_edges(n_, edge_count, a.data(), b.data(), f.data(), w.data(), nullptr, &g, dims),
           "set_nweights");
     grid_.reset(new GridGraph(g, dims[0], dims[1], dims[2]));
-    if (!pending_s_.empty()) {
-      grid_->set_tweights(pending_s_.data(), pending_t_.data());
-      pending_s_.clear();
-      pending_t_.clear();
-    }
+    // t-links set earlier (the reference accepts them in either order) apply
+    // to the new grid as well
+    if (!tlink_s_.empty()) grid_->set_tweights(tlink_s_.data(), tlink_t_.data());
   }
 
   void set_tweights(const EdgeWeight* capSource, const EdgeWeight* capSink) {
-    std::vector<int32_t> s = detail::to_i32(capSource, (size_t)n_, "set_tweights");
-    std::vector<int32_t> t = detail::to_i32(capSink, (size_t)n_, "set_tweights");
-    if (!grid_) {  // the reference accepts t-links before n-links
-      pending_s_.swap(s);
-      pending_t_.swap(t);
-      return;
-    }
-    grid_->set_tweights(s.data(), t.data());
+    tlink_s_ = detail::to_i32(capSource, (size_t)n_, "set_tweights");
+    tlink_t_ = detail::to_i32(capSink, (size_t)n_, "set_tweights");
+    if (grid_) grid_->set_tweights(tlink_s_.data(), tlink_t_.data());
   }
 
   TFlow max_flow() {
@@ -239,7 +234,7 @@ class Graph {
 
   int n_ = 0;
   GridPtr grid_;
-  std::vector<int32_t> pending_s_, pending_t_;
+  std::vector<int32_t> tlink_s_, tlink_t_;  // host copy of the last t-links
 };
 
 }  // namespace cgc
