@@ -52,7 +52,7 @@ struct InstGeo {
   int32_t X, Y, Z;      // voxel extents
   int32_t TX, TY, TZ;   // tile extents
   int32_t tile_base;    // first tile of the instance
-  int32_t hdead;        // heights >= hdead cannot reach the sink (voxel count)
+  int32_t hdead;        // heights >= hdead cannot reach the sink (voxel count + 1)
 };
 
 struct DevPool {
@@ -82,5 +82,22 @@ struct DevPool {
 };
 
 __host__ __device__ inline int dir_axis(int d) { return d >> 1; }
+
+// parameters of the persistent solve kernel
+struct SolveParams {
+  int L;                 // pulses per tile visit (per region-relabel round)
+  int R;                 // region-relabel rounds per tile visit (0: pulses only)
+  int K;                 // sweep pairs between global relabels
+  int64_t max_sweeps;    // cap on sweeps (parity steps)
+  uint64_t limit_ns;     // bounded barrier wait
+};
+
+// kernels of cgc_engine.cu launched from other translation units
+__global__ void k_put_tlinks(DevPool P, int inst, const int32_t* __restrict__ capS, const int32_t* __restrict__ capT);
+__global__ void k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __restrict__ fwd,
+                             const int32_t* __restrict__ bwd);
+__global__ void k_prepare(DevPool P);
+__global__ void k_solve(DevPool P, SolveParams prm);
+__global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);
 
 }  // namespace cgc

@@ -225,13 +225,6 @@ __device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
 
 __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }
 
-struct SolveParams {
-  int L;                 // pulses per tile visit (per region-relabel round)
-  int R;                 // region-relabel rounds per tile visit (0: pulses only)
-  int K;                 // sweep pairs between global relabels
-  int64_t max_sweeps;    // cap on sweeps (parity steps)
-  uint64_t limit_ns;     // bounded barrier wait
-};
 
 union SolveShared {
   SweepShared sw;
@@ -421,8 +414,8 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
     G.TX = (X + 7) / 8; G.TY = (Y + 7) / 8; G.TZ = (Z + 7) / 8;
     G.tile_base = (int32_t)T;
     const int64_t n = (int64_t)X * Y * Z;
-    if (n >= (int64_t)INF) return fail(CGC_ERR_ARG, "create: instance too large for int32 heights");
-    G.hdead = (int32_t)n;
+    if (n + 1 >= (int64_t)INF) return fail(CGC_ERR_ARG, "create: instance too large for int32 heights");
+    G.hdead = (int32_t)(n + 1);  // a distance to the sink is at most n (a path through every voxel)
     T += (int64_t)G.TX * G.TY * G.TZ;
     if (T > (int64_t)1 << 30) return fail(CGC_ERR_ARG, "create: too many tiles");
     p->maxN = std::max(p->maxN, n);

@@ -206,3 +206,53 @@ def test_sparse_terminals_match_oracle(seed, policy):
     f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
     flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, bwd, POLICIES[policy])
     assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
+
+
+@pytest.mark.parametrize("policy", ["default", "host_loop", "no_region"])
+@pytest.mark.parametrize("axis,n", [(0, 2), (0, 9), (0, 16), (0, 40), (1, 17), (2, 24), (0, 64)])
+def test_chain_through_every_voxel(axis, n, policy):
+    """A 1-D chain with the source at one end and the sink at the other: the
+    first voxel's distance to the sink is the voxel count itself."""
+    dims = [1, 1, 1]
+    dims[axis] = n
+    X, Y, Z = dims
+    capS = np.zeros(n, np.int32)
+    capT = np.zeros(n, np.int32)
+    capS[0] = 50
+    capT[-1] = 50
+    chain = np.full(n, 9, np.int32)
+    chain[(n - 1) // 2] = 3
+    chain[-1] = 0
+    z = np.zeros(n, np.int32)
+    fwd = [z, z, z]
+    fwd[axis] = chain
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd)
+    flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, None, POLICIES[policy])
+    assert f0 == 3
+    assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
+
+
+def test_snake_path_longer_than_a_tile():
+    """One long winding path through a 2-D grid (every voxel on it): the
+    distance to the sink is the voxel count, far beyond a tile."""
+    X, Y = 24, 16
+    N = X * Y
+    order = [(x if y % 2 == 0 else X - 1 - x, y) for y in range(Y) for x in range(X)]
+    fx = np.zeros((Y, X), np.int32)
+    fy = np.zeros((Y, X), np.int32)
+    for (x0, y0), (x1, y1) in zip(order, order[1:]):
+        if y0 == y1:
+            fx[y0, min(x0, x1)] = 7
+        else:
+            fy[min(y0, y1), x0] = 7
+    capS = np.zeros((Y, X), np.int32)
+    capT = np.zeros((Y, X), np.int32)
+    capS[order[0][1], order[0][0]] = 100
+    capT[order[-1][1], order[-1][0]] = 100
+    z = np.zeros(N, np.int32)
+    fwd = [fx.reshape(-1), fy.reshape(-1), z]
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, 1, capS.reshape(-1), capT.reshape(-1), fwd)
+    assert f0 == 7
+    for pol in (None, Policy(persistent=-1), Policy(region_relabels=-1, local_pulses=2)):
+        flow, smin, treach, _ = solve(X, Y, 1, capS.reshape(-1), capT.reshape(-1), fwd, None, pol)
+        assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
