@@ -84,6 +84,8 @@ SIGNATURES = {
     "cgc_grid_get_segments_device": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
     "cgc_grid_get_residuals": (C.c_int, [VP, C.POINTER(VP), VP, VP]),
     "cgc_grid_stats": (C.c_int, [VP, C.POINTER(Stats)]),
+    "cgc_grid_maxflow_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, VP, VP, C.POINTER(VP), C.POINTER(VP),
+                                           C.POINTER(Options), VP, P64, VP, VP]),
     "cgc_batch_create": (C.c_int, [C.c_int32, VP, VP, C.POINTER(VP)]),
     "cgc_batch_destroy": (C.c_int, [VP]),
     "cgc_batch_set_tlinks": (C.c_int, [VP, C.c_int32, VP, VP]),

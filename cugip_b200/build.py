@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcgc.so")
 
-SOURCES = ["cgc_engine.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
+SOURCES = ["cgc_engine.cu", "cgc_noalloc.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
 HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h"]
 
 NVCC_FLAGS = [

@@ -166,6 +166,27 @@ int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, in
 
 int cgc_grid_stats(cgc_grid* g, cgc_stats* out);
 
+/* ---- allocation-free solve of a small grid ---------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory: processes whose device memory belongs to another allocator (a
+ * framework's caching pool or a fixed budget) and real-time loops that cannot
+ * take the device-wide synchronisation of cudaMalloc / cudaFree.  The caller
+ * passes device inputs (capS, capT and the fwd/bwd n-link planes of each axis
+ * as in cgc_grid_set_nlinks; a NULL axis means zero capacity) and device
+ * outputs (source_side / sink_side: X*Y*Z bytes of 1/0, each may be NULL); the
+ * flow is written to the host int64 *flow and the call blocks until done.
+ * All working state lives in one static device array that every GPU loading
+ * this library holds until exit, so the grid may hold at most
+ * CGC_NOALLOC_MAX_VOXELS voxels after rounding each extent up to a multiple of
+ * 8 (64^3 fits); larger grids return CGC_ERR_ARG.  The first call on a device
+ * sets that device up and should come before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race and must not be issued. */
+#define CGC_NOALLOC_MAX_VOXELS 262144
+int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const int32_t* capS, const int32_t* capT,
+                             const int32_t* const fwd[3], const int32_t* const bwd[3],
+                             const cgc_options* opts, void* stream, int64_t* flow,
+                             uint8_t* source_side, uint8_t* sink_side);
+
 /* ---- batch of grids (uneven sizes, one solve) ----------------------------
  * Replaces nothing in the reference (it solves one graph per Graph object);
  * all instances share one tile pool and are solved by the same launches. */
