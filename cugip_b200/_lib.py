@@ -35,7 +35,8 @@ class CgcError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("struct_size", C.c_int32), ("local_pulses", C.c_int32), ("sweeps_per_relabel", C.c_int32),
                 ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
-                ("region_relabels", C.c_int32), ("reserved", C.c_int32 * 9)]
+                ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class Stats(C.Structure):
@@ -84,6 +85,8 @@ SIGNATURES = {
     "cgc_grid_get_segments_device": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
     "cgc_grid_get_residuals": (C.c_int, [VP, C.POINTER(VP), VP, VP]),
     "cgc_grid_stats": (C.c_int, [VP, C.POINTER(Stats)]),
+    "cgc_grid_trace": (C.c_int, [VP, VP, C.c_int32, P32]),
+    "cgc_batch_trace": (C.c_int, [VP, VP, C.c_int32, P32]),
     "cgc_grid_maxflow_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, VP, VP, C.POINTER(VP), C.POINTER(VP),
                                            C.POINTER(Options), VP, P64, VP, VP]),
     "cgc_batch_create": (C.c_int, [C.c_int32, VP, VP, C.POINTER(VP)]),
@@ -123,7 +126,7 @@ def check(rc: int) -> None:
 
 
 def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
-            persistent: int = 0, region_relabels: int = 0) -> Options:
+            persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0, ctas_per_sm: int = 0) -> Options:
     o = Options()
     o.struct_size = C.sizeof(Options)
     o.local_pulses = local_pulses
@@ -132,4 +135,6 @@ def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 
     o.max_sweeps = max_sweeps
     o.persistent = persistent
     o.region_relabels = region_relabels
+    o.stall_sweeps = stall_sweeps
+    o.ctas_per_sm = ctas_per_sm
     return o

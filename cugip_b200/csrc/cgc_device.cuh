@@ -36,17 +36,26 @@ enum Counter {
   C_SW0 = 3,       // 4 sweep worklists
   C_ACT = 7,       // active tiles after the last global relabel
   C_ROUNDS = 8,    // BFS rounds executed
+  C_SINKT0 = 9,    // 3 slots: tiles that delivered flow to the sink in a sweep
   C_NCOUNTERS = 16
 };
 
 // statistics in DevPool::stats (unsigned long long)
 enum Stat {
   S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5,
-  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_NSTATS = 12
+  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_NSTATS = 12
 };
 
+// phase trace records written by the persistent solve (two words each):
+//   word 0 = kind << 56 | index << 24 | tiles, word 1 = ns since the launch
+enum TraceKind { TR_BFS_ROUND = 1, TR_RELABEL_DONE = 2, TR_SWEEP = 3, TR_REACH_ROUND = 4 };
+constexpr int TRACE_CAP = 16384;
+
 // BFS seed summary of a tile (DevPool::tflag)
-enum TileFlag { TF_ALL_SEED = 1, TF_FACE0 = 2 /* bits 1..6: a seed on face d */, TF_HAS_SEED = 128 };
+enum TileFlag {
+  TF_ALL_SEED = 1, TF_FACE0 = 2 /* bits 1..6: a seed on face d */, TF_HAS_SEED = 128,
+  TF_DEAD = 256 /* every voxel cannot reach the sink: stays so for the rest of the solve */
+};
 
 struct InstGeo {
   int32_t X, Y, Z;      // voxel extents
@@ -69,7 +78,7 @@ struct DevPool {
   const int32_t* tinst; // T: instance of the tile
   const uint8_t* tpar;  // T: (tx+ty+tz)&1
   uint8_t* act;         // T: tile holds an active voxel (e>0, h<INF)
-  uint8_t* tflag;       // T: BFS seed summary (TF_* bits)
+  uint16_t* tflag;      // T: BFS seed summary (TF_* bits)
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
   uint32_t* stamp_sw;   // T: last sweep the tile was queued for
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
@@ -79,6 +88,7 @@ struct DevPool {
   unsigned long long* stats;  // S_NSTATS
   int32_t* err;         // first error code raised on the device
   uint32_t* bar;        // grid barrier: [0] arrivals, [1] generation
+  unsigned long long* trace;  // 2*TRACE_CAP words of phase records (may be null)
 };
 
 __host__ __device__ inline int dir_axis(int d) { return d >> 1; }
@@ -88,6 +98,7 @@ struct SolveParams {
   int L;                 // pulses per tile visit (per region-relabel round)
   int R;                 // region-relabel rounds per tile visit (0: pulses only)
   int K;                 // sweep pairs between global relabels
+  int stall;             // relabel after this many sweeps without sink flow (0: never)
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
 };

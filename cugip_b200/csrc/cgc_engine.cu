@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   if (bad) raise_error(P, CGC_ERR_OVERFLOW);
   P.e[g] = e;
   P.rT[g] = rT;
-  P.h[g] = INF;
+  P.h[g] = 0;  // no label yet (INF would read as "dead" to the first global relabel)
   P.rmask[g] = (uint8_t)m;
   P.reach[g] = 0;
   const long long tot = block_sum64((long long)mcap, red);
@@ -233,8 +233,7 @@ union SolveShared {
 };
 
 // The whole solve in one cooperative launch.
-__global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
-  __shared__ SolveShared S;
+__device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, SolveShared& S) {
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
   int32_t* const sl[4] = {P.lists + 3 * P.T, P.lists + 4 * P.T, P.lists + 5 * P.T, P.lists + 6 * P.T};
@@ -246,6 +245,16 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   long long rounds = 0, relabels = 0;
   unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0;
   uint64_t tmark = globaltimer_ns();
+  const uint64_t t_launch = tmark;
+  int ntrace = 0;
+  // block 0 records one phase step (after the barrier that ended it)
+  auto record = [&](unsigned long long kind, long long index, int tiles) {
+    if (b == 0 && tid == 0 && P.trace && ntrace < TRACE_CAP) {
+      P.trace[2 * ntrace] = (kind << 56) | ((unsigned long long)(index & 0xffffffffll) << 24) | (unsigned)(tiles & 0xffffff);
+      P.trace[2 * ntrace + 1] = globaltimer_ns() - t_launch;
+      ++ntrace;
+    }
+  };
   auto lap = [&](unsigned long long& acc) {
     const uint64_t now = globaltimer_ns();
     acc += now - tmark;
@@ -256,6 +265,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     if (b == 0 && tid == 0) {
       bc[0] = bc[1] = bc[2] = 0;
       sc[0] = sc[1] = sc[2] = sc[3] = 0;
+      P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
     }
     if (!grid_sync(P, prm.limit_ns)) return;
     for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs);
@@ -270,6 +280,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
       for (int i = b; i < n; i += G) bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
       ++k;
       if (!grid_sync(P, prm.limit_ns)) return;
+      record(TR_BFS_ROUND, rounds + k, n);
     }
     bfs_id += k + 1;
     rounds += k;
@@ -286,21 +297,33 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     }
     if (!grid_sync(P, prm.limit_ns)) return;
     const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));
+    record(TR_RELABEL_DONE, relabels, nact);
     if (nact == 0) break;
     if (sweeps >= prm.max_sweeps) {
       if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
       break;
     }
     // ------------------------------------------------ sweeps
+    int idle = 0;  // consecutive sweeps in which no tile delivered flow to the sink
     for (int j = 0; j < 2 * prm.K; ++j, ++s) {
       const int n = ld_cnt(sc + (s & 3));
       if (n == 0 && ld_cnt(sc + ((s + 1) & 3)) == 0) break;
-      if (b == 0 && tid == 0) sc[(s + 3) & 3] = 0;
+      if (b == 0 && tid == 0) {
+        sc[(s + 3) & 3] = 0;
+        P.cnt[C_SINKT0 + (int)((s + 1) % 3)] = 0;
+      }
       for (int i = b; i < n; i += G)
         sweep_tile<true>(P, __ldcg(sl[s & 3] + i), prm.L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3));
+                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), P.cnt + C_SINKT0 + (int)(s % 3));
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
+      record(TR_SWEEP, sweeps, n);
+      // Early relabel: after stall consecutive non-empty sweeps of each parity
+      // delivered no flow to the sink.  Empty sweeps do not count, so every
+      // cycle performs at least one push or relabel; labels never decrease
+      // (an exact relabel only raises valid labels), so the solve still ends.
+      if (n > 0) idle = ld_cnt(P.cnt + C_SINKT0 + (int)(s % 3)) ? 0 : idle + 1;
+      if (prm.stall > 0 && idle >= 2 * prm.stall) { ++s; break; }
     }
     lap(ns_sweep);
   }
@@ -318,6 +341,7 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     for (int i = b; i < n; i += G) reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
     ++k;
     if (!grid_sync(P, prm.limit_ns)) return;
+    record(TR_REACH_ROUND, k, n);
   }
   if (b == 0 && tid == 0) {
     P.stats[S_SWEEPS] = (unsigned long long)sweeps;
@@ -327,7 +351,19 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
     P.stats[S_NS_BFS] = ns_bfs;
     P.stats[S_NS_SWEEP] = ns_sweep;
     P.stats[S_NS_REACH] = ns_reach;
+    P.stats[S_TRACE_N] = (unsigned long long)ntrace;
   }
+}
+
+// The solve kernel at 2 CTAs per SM (64 registers) and at 3 (40 registers,
+// a few spills).
+__global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_body(P, prm, S);
+}
+__global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_body(P, prm, S);
 }
 
 // Output kernels (linear layout of one instance).
@@ -374,6 +410,7 @@ struct Pool {
   bool solved = false;
   int sms = 148;
   int coop_blocks = 0;           // co-resident CTAs of k_solve
+  int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
   int sweep_blocks = 0;
   cgc_stats st{};
   std::vector<int64_t> flows;
@@ -440,7 +477,7 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   const int64_t o_ti = off; off += al(T * 4);
   const int64_t o_tp = off; off += al(T);
   const int64_t o_act = off; off += al(T);
-  const int64_t o_tf = off; off += al(T);
+  const int64_t o_tf = off; off += al(T * 2);
   const int64_t o_sb = off; off += al(T * 4);
   const int64_t o_ss = off; off += al(T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
@@ -450,6 +487,7 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   const int64_t o_st = off; off += al(S_NSTATS * 8);
   const int64_t o_err = off; off += al(4);
   const int64_t o_bar = off; off += al(8);
+  const int64_t o_tr = off; off += al(2 * TRACE_CAP * 8);
   CGC_CUDA(cudaMalloc(&p->dbuf, off));
   CGC_CUDA(cudaMemsetAsync(p->dbuf, 0, off, p->stream));
   char* base = (char*)p->dbuf;
@@ -458,10 +496,11 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   d.e = (int32_t*)(base + o_e); d.h = (int32_t*)(base + o_h); d.rT = (int32_t*)(base + o_rT);
   d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
   d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
-  d.act = (uint8_t*)(base + o_act); d.tflag = (uint8_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
+  d.act = (uint8_t*)(base + o_act); d.tflag = (uint16_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
   d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
   d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
   d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
+  d.trace = (unsigned long long*)(base + o_tr);
 
   // tile tables
   std::vector<int32_t> nbr(6 * (size_t)T, -1), ti((size_t)T);
@@ -497,6 +536,9 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   int occ = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, 512, 0));
   p->coop_blocks = std::max(1, occ) * p->sms;
+  int occ3 = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_solve3, 512, 0));
+  p->coop_blocks3 = std::max(1, occ3) * p->sms;
   int occ2 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_sweep_list, 512, 0));
   p->sweep_blocks = std::max(1, occ2) * p->sms;
@@ -550,9 +592,11 @@ static cgc_options resolve_options(const cgc_options* o) {
   r.local_pulses = 16;
   r.sweeps_per_relabel = 8;
   r.schedule = CGC_SCHED_PARITY;
-  r.max_sweeps = 1 << 20;
+  r.max_sweeps = 1 << 17;
   r.persistent = 1;
   r.region_relabels = 1;
+  r.stall_sweeps = 0;
+  r.ctas_per_sm = 2;
   if (o) {
     if (o->local_pulses > 0) r.local_pulses = std::min(o->local_pulses, 64);
     if (o->sweeps_per_relabel > 0) r.sweeps_per_relabel = o->sweeps_per_relabel;
@@ -560,6 +604,8 @@ static cgc_options resolve_options(const cgc_options* o) {
     if (o->max_sweeps > 0) r.max_sweeps = o->max_sweeps;
     if (o->persistent) r.persistent = o->persistent;
     if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
+    if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
+    if (o->ctas_per_sm == 2 || o->ctas_per_sm == 3) r.ctas_per_sm = o->ctas_per_sm;
   }
   return r;
 }
@@ -628,11 +674,14 @@ static int pool_solve(Pool& p, const cgc_options* opts) {
     prm.L = o.local_pulses;
     prm.R = o.region_relabels;
     prm.K = o.sweeps_per_relabel;
+    prm.stall = o.stall_sweeps;
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
     void* args[] = {(void*)&d, (void*)&prm};
     CGC_CUDA(cudaEventRecord(evk0, p.stream));
-    CGC_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve, dim3(p.coop_blocks), dim3(512), args, 0, p.stream));
+    const bool three = o.ctas_per_sm == 3;
+    CGC_CUDA(cudaLaunchCooperativeKernel(three ? (const void*)k_solve3 : (const void*)k_solve,
+                                         dim3(three ? p.coop_blocks3 : p.coop_blocks), dim3(512), args, 0, p.stream));
     note_launch();
     CGC_CUDA(cudaEventRecord(evk1, p.stream));
   } else {
@@ -742,6 +791,18 @@ static int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* res
   return ok();
 }
 
+static int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count) {
+  if (!p.solved) return fail(CGC_ERR_STATE, "trace: call maxflow first");
+  unsigned long long n = 0;
+  CGC_CUDA(cudaMemcpy(&n, p.dp.stats + S_TRACE_N, 8, cudaMemcpyDeviceToHost));
+  *count = (int32_t)n;
+  if (out && cap > 0) {
+    const int64_t m = std::min<int64_t>((int64_t)n, cap);
+    CGC_CUDA(cudaMemcpy(out, p.dp.trace, (size_t)m * 16, cudaMemcpyDeviceToHost));
+  }
+  return ok();
+}
+
 }  // namespace cgc
 
 // ===========================================================================
@@ -817,6 +878,14 @@ int cgc_grid_get_segments_device(cgc_grid* g, int which, uint8_t* out, uint8_t m
 int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, int32_t* excess) {
   if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
   return cgc::pool_residuals(*g->p, 0, res, resT, excess);
+}
+int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count) {
+  if (!g || !count) return cgc::fail(CGC_ERR_ARG, "null argument");
+  return cgc::pool_trace(*g->p, out, cap, count);
+}
+int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count) {
+  if (!b || !count) return cgc::fail(CGC_ERR_ARG, "null argument");
+  return cgc::pool_trace(*b->p, out, cap, count);
 }
 int cgc_grid_stats(cgc_grid* g, cgc_stats* out) {
   if (!g || !out) return cgc::fail(CGC_ERR_ARG, "null argument");

@@ -151,7 +151,8 @@ struct ReachShared {
 template <bool APPEND>
 __device__ void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
-                           const uint32_t id_self, int32_t* list_self, int32_t* cnt_self) {
+                           const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
+                           int32_t* sink_tiles = nullptr) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -277,7 +278,10 @@ __device__ void sweep_tile(const DevPool& P, const int t, const int L, const int
   const long long total = block_sum64((long long)sink, S.red);
   if (l == 0) {
     P.act[t] = (uint8_t)(still ? 1 : 0);
-    if (total) atomicAdd(P.flow + inst, (unsigned long long)total);
+    if (total) {
+      atomicAdd(P.flow + inst, (unsigned long long)total);
+      if (sink_tiles) atomicAdd(sink_tiles, 1);
+    }
     atomicAdd(P.stats + S_TILES_SWEPT, 1ull);
     atomicAdd(P.stats + S_PULSES, (unsigned long long)pulses);
     if (APPEND && still) {
@@ -308,6 +312,15 @@ __device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
   const int64_t g = (int64_t)t * TV + l;
   const unsigned rm = __ldcg(P.rmask + g);
   const bool seed = (rm & 64u) != 0;
+  // A tile whose voxels were all found unable to reach the sink stays so
+  // (dead vertices neither receive nor send flow, and all their residual
+  // neighbours are dead), so it keeps INF and is never visited again.
+  // Heights are 0 before the first relabel of a solve.
+  const int dead = __syncthreads_and(__ldcg(P.h + g) == INF);
+  if (dead) {
+    if (l == 0) { P.tflag[t] = TF_DEAD; P.act[t] = 0; }
+    return;
+  }
   P.h[g] = seed ? 1 : INF;
   if (l == 0) S.flags = 0;
   __syncthreads();
@@ -317,7 +330,7 @@ __device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
   int act = 0;
   if (all_seed) act = __syncthreads_or((rm & 128u) != 0);
   if (l == 0) {
-    P.tflag[t] = (uint8_t)(S.flags | (all_seed ? TF_ALL_SEED : 0));
+    P.tflag[t] = (uint16_t)(S.flags | (all_seed ? TF_ALL_SEED : 0));
     P.act[t] = (uint8_t)(act ? 1 : 0);
   }
   __syncthreads();
@@ -330,12 +343,12 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
   bool q = false;
   if (t < P.T) {
     const int f = __ldcg(P.tflag + t);
-    if (!(f & TF_ALL_SEED)) {
+    if (!(f & (TF_ALL_SEED | TF_DEAD))) {
       q = (f & TF_HAS_SEED) != 0;
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         const int nt = __ldcg(P.nbr + d * P.T + t);
-        if (nt >= 0 && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1)) q = true;
+        if (nt >= 0 && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1)) q = true;  // dead tiles have no seed bits
       }
     }
     if (q) P.stamp_bfs[t] = id0;
@@ -347,6 +360,7 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
 // until the tile is stable; re-queue face neighbours whose halo changed.
 __device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
                          int32_t* list_next, int32_t* cnt_next) {
+  if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;

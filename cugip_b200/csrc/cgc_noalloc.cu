@@ -53,7 +53,7 @@ constexpr int64_t kOffTinst = kOffNbr + al256(6 * kMaxTiles * 4);
 constexpr int64_t kOffTpar = kOffTinst + al256(kMaxTiles * 4);
 constexpr int64_t kOffAct = kOffTpar + al256(kMaxTiles);
 constexpr int64_t kOffTflag = kOffAct + al256(kMaxTiles);
-constexpr int64_t kOffStampB = kOffTflag + al256(kMaxTiles);
+constexpr int64_t kOffStampB = kOffTflag + al256(kMaxTiles * 2);
 constexpr int64_t kOffStampS = kOffStampB + al256(kMaxTiles * 4);
 constexpr int64_t kOffLists = kOffStampS + al256(kMaxTiles * 4);
 constexpr int64_t kOffCnt = kOffLists + al256(7 * kMaxTiles * 4);
@@ -156,7 +156,7 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   P.r = (int32_t*)(base + kOffR);  // planes are kMaxVoxels apart below
   P.rmask = base + kOffRmask; P.reach = base + kOffReach;
   P.nbr = (const int32_t*)(base + kOffNbr); P.tinst = (const int32_t*)(base + kOffTinst);
-  P.tpar = base + kOffTpar; P.act = base + kOffAct; P.tflag = base + kOffTflag;
+  P.tpar = base + kOffTpar; P.act = base + kOffAct; P.tflag = (uint16_t*)(base + kOffTflag);
   P.stamp_bfs = (uint32_t*)(base + kOffStampB); P.stamp_sw = (uint32_t*)(base + kOffStampS);
   P.lists = (int32_t*)(base + kOffLists); P.cnt = (int32_t*)(base + kOffCnt);
   P.flow = (unsigned long long*)(base + kOffFlow); P.geo = (const InstGeo*)(base + kOffGeo);
@@ -192,7 +192,8 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   prm.L = o.local_pulses > 0 ? (o.local_pulses < 64 ? o.local_pulses : 64) : 16;
   prm.R = o.region_relabels < 0 ? 0 : (o.region_relabels > 0 ? (o.region_relabels < 16 ? o.region_relabels : 16) : 1);
   prm.K = o.sweeps_per_relabel > 0 ? o.sweeps_per_relabel : 8;
-  prm.max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : (1 << 20);
+  prm.stall = o.stall_sweeps > 0 ? o.stall_sweeps : 0;
+  prm.max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : (1 << 17);
   prm.limit_ns = 20ull * 1000000000ull;
   void* args[] = {(void*)&P, (void*)&prm};
   // a preparation error (overflowing capacities) makes every CTA leave at its

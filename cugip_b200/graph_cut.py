@@ -55,8 +55,11 @@ class Policy:
     """Runtime counterpart of GraphCutPolicy (detail/graph_cut_policies.hpp:23-89)."""
 
     def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0,
-                 max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0):
+                 max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0,
+                 ctas_per_sm: int = 0):
+        self.ctas_per_sm = ctas_per_sm
         self.region_relabels = region_relabels
+        self.stall_sweeps = stall_sweeps
         self.local_pulses = local_pulses
         self.sweeps_per_relabel = sweeps_per_relabel
         self.schedule = schedule
@@ -65,7 +68,7 @@ class Policy:
 
     def options(self) -> _lib.Options:
         return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
-                            self.persistent, self.region_relabels)
+                            self.persistent, self.region_relabels, self.stall_sweeps, self.ctas_per_sm)
 
 
 class GridGraph:
@@ -164,6 +167,25 @@ class GridGraph:
         s = _lib.Stats()
         check(self._lib.cgc_grid_stats(self._h, C.byref(s)))
         return s.as_dict()
+
+    def trace(self) -> list:
+        return _read_trace(self._lib.cgc_grid_trace, self._h)
+
+
+TRACE_KINDS = {1: "bfs_round", 2: "relabel_done", 3: "sweep", 4: "reach_round"}
+
+
+def _read_trace(fn, handle) -> list:
+    n = C.c_int32()
+    check(fn(handle, None, 0, C.byref(n)))
+    buf = np.zeros(2 * max(n.value, 1), dtype=np.int64)
+    check(fn(handle, buf.ctypes.data_as(C.c_void_p), n.value, C.byref(n)))
+    out = []
+    for i in range(n.value):
+        w = int(buf[2 * i]) & 0xFFFFFFFFFFFFFFFF
+        out.append({"kind": TRACE_KINDS.get(w >> 56, w >> 56), "index": (w >> 24) & 0xFFFFFFFF,
+                    "tiles": w & 0xFFFFFF, "ns": int(buf[2 * i + 1])})
+    return out
 
 
 class Graph:
@@ -281,3 +303,6 @@ class Batch:
         s = _lib.Stats()
         check(self._lib.cgc_batch_stats(self._h, C.byref(s)))
         return s.as_dict()
+
+    def trace(self) -> list:
+        return _read_trace(self._lib.cgc_batch_trace, self._h)

@@ -73,10 +73,12 @@ typedef struct cgc_options {
   int32_t local_pulses;       /* push/relabel pulses per tile visit (1..64), default 16 */
   int32_t sweeps_per_relabel; /* sweep pairs between global relabels, default 8 */
   int32_t schedule;           /* CGC_SCHED_* (default parity) */
-  int32_t max_sweeps;         /* safety cap on sweep pairs, default 1<<20 */
+  int32_t max_sweeps;         /* safety cap on sweeps, default 1<<17 */
   int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
   int32_t region_relabels;    /* region-relabel rounds per tile visit (default 1, -1 = none) */
-  int32_t reserved[9];
+  int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
+  int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers) or 3 (40 registers) */
+  int32_t reserved[7];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */
@@ -166,6 +168,14 @@ int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, in
 
 int cgc_grid_stats(cgc_grid* g, cgc_stats* out);
 
+/* Phase trace of the last persistent solve (extends the reference's trace
+ * hooks, graph_cut.hpp:26-45, with per-step detail): *count receives the
+ * number of records; up to `cap` records of two int64 each are copied to out:
+ * word 0 = kind << 56 | index << 24 | tiles (kind 1 = BFS round, 2 = global
+ * relabel done (tiles = active tiles), 3 = sweep, 4 = reachability round),
+ * word 1 = nanoseconds since the launch. */
+int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count);
+
 /* ---- allocation-free solve of a small grid ---------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory: processes whose device memory belongs to another allocator (a
@@ -198,6 +208,7 @@ int cgc_batch_set_nlinks(cgc_batch* b, int32_t i, int axis, const int32_t* fwd, 
 int cgc_batch_maxflow(cgc_batch* b, const cgc_options* opts, int64_t* flows /* count */);
 int cgc_batch_get_segments(cgc_batch* b, int32_t i, int which, uint8_t* out, uint8_t mask, uint8_t background);
 int cgc_batch_stats(cgc_batch* b, cgc_stats* out);
+int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count);
 
 /* ---- synthetic inputs ------------------------------------------------------
  * Deterministic capacity volumes for the benchmark workloads (x-fastest,

@@ -27,6 +27,8 @@ POLICIES = {
     "no_region": Policy(region_relabels=-1),
     "R3_L2": Policy(local_pulses=2, region_relabels=3, sweeps_per_relabel=2),
     "host_R2": Policy(region_relabels=2, persistent=-1),
+    "stall1_K64": Policy(stall_sweeps=1, sweeps_per_relabel=64),
+    "stall3_L2": Policy(stall_sweeps=3, local_pulses=2, sweeps_per_relabel=16),
 }
 
 
