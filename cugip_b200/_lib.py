@@ -96,6 +96,17 @@ SIGNATURES = {
     "cgc_batch_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),
     "cgc_batch_get_segments": (C.c_int, [VP, C.c_int32, C.c_int, VP, C.c_uint8, C.c_uint8]),
     "cgc_batch_stats": (C.c_int, [VP, C.POINTER(Stats)]),
+    "cgc_batch_bind_inputs": (C.c_int, [VP, C.c_int32, VP, VP, C.POINTER(VP), C.POINTER(VP)]),
+    "cgc_batch_bind_outputs": (C.c_int, [VP, C.c_int32, VP, VP]),
+    "cgc_batch_enqueue": (C.c_int, [VP, C.POINTER(Options), VP]),
+    "cgc_batch_graph_create": (C.c_int, [VP, C.POINTER(Options), VP]),
+    "cgc_batch_graph_launch": (C.c_int, [VP]),
+    "cgc_batch_wait": (C.c_int, [VP, P64]),
+    "cgc_grid_autotune": (C.c_int, [VP, C.POINTER(Options), C.c_int32, C.c_int32, C.POINTER(Options),
+                                    C.POINTER(C.c_double)]),
+    "cgc_batch_autotune": (C.c_int, [VP, C.POINTER(Options), C.c_int32, C.c_int32, C.POINTER(Options),
+                                     C.POINTER(C.c_double)]),
+    "cgc_autotune_lookup": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(Options)]),
     "cgc_volume_preset": (C.c_int, [C.c_int, C.c_int32, C.POINTER(VolumeSpec)]),
     "cgc_volume_generate": (C.c_int, [C.POINTER(VolumeSpec), VP, VP, VP, VP, VP, VP]),
 }

@@ -109,6 +109,7 @@ __global__ void k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __res
                              const int32_t* __restrict__ bwd);
 __global__ void k_prepare(DevPool P);
 __global__ void k_solve(DevPool P, SolveParams prm);
+__global__ void k_solve3(DevPool P, SolveParams prm);
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);
 
 }  // namespace cgc

@@ -23,12 +23,13 @@
 #include "cgc.h"
 #include "cgc_internal.h"
 #include "cgc_kernels.cuh"
+#include "cgc_pool.h"
 
 namespace cgc {
 
 static thread_local std::string g_last_error;
-static std::atomic<long long> g_launches{0};
-static inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -39,13 +40,6 @@ int ok() {
   return CGC_OK;
 }
 
-#define CGC_CUDA(call)                                                                      \
-  do {                                                                                      \
-    cudaError_t e_ = (call);                                                                \
-    if (e_ != cudaSuccess)                                                                  \
-      return ::cgc::fail(e_ == cudaErrorMemoryAllocation ? CGC_ERR_OOM : CGC_ERR_CUDA,      \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                      \
-  } while (0)
 
 // ===========================================================================
 // kernels
@@ -393,36 +387,7 @@ __global__ void k_unpermute(DevPool P, int inst, const int32_t* plane, int32_t* 
 // host side
 // ===========================================================================
 
-struct Pool {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int ninst = 0;
-  std::vector<InstGeo> geo;
-  std::vector<uint32_t> uploaded;  // bit 0 tlinks, bits 1..3 axes
-  int64_t maxN = 0;
-  int32_t T = 0;
-  int64_t Np = 0;
-  DevPool dp{};
-  void* dbuf = nullptr;          // all device state
-  int32_t* staging = nullptr;    // 2*maxN int32
-  uint8_t* seg = nullptr;        // maxN bytes
-  int32_t* pinned_cnt = nullptr; // host-pinned counters
-  bool solved = false;
-  int sms = 148;
-  int coop_blocks = 0;           // co-resident CTAs of k_solve
-  int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
-  int sweep_blocks = 0;
-  cgc_stats st{};
-  std::vector<int64_t> flows;
-  ~Pool() {
-    if (dbuf) cudaFree(dbuf);
-    if (staging) cudaFree(staging);
-    if (seg) cudaFree(seg);
-    if (pinned_cnt) cudaFreeHost(pinned_cnt);
-  }
-};
-
-static int check_device_error(Pool& p, const char* where) {
+int check_device_error(Pool& p, const char* where) {
   int32_t err = 0;
   CGC_CUDA(cudaMemcpyAsync(&err, p.dp.err, sizeof(int32_t), cudaMemcpyDeviceToHost, p.stream));
   CGC_CUDA(cudaStreamSynchronize(p.stream));
@@ -435,7 +400,7 @@ static int check_device_error(Pool& p, const char* where) {
   return fail(err, std::string(where) + ": " + what);
 }
 
-static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
+int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   if (!out || count <= 0 || !ext) return fail(CGC_ERR_ARG, "create: bad arguments");
   std::unique_ptr<Pool> p(new (std::nothrow) Pool());
   if (!p) return fail(CGC_ERR_OOM, "create: host allocation");
@@ -547,7 +512,7 @@ static int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** o
   return ok();
 }
 
-static int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host) {
+int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host) {
   if (inst < 0 || inst >= p.ninst || !capS || !capT) return fail(CGC_ERR_ARG, "set_tlinks: bad arguments");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
@@ -564,7 +529,7 @@ static int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t
   return ok();
 }
 
-static int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host) {
+int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host) {
   if (inst < 0 || inst >= p.ninst || axis < 0 || axis > 2 || !fwd || !bwd)
     return fail(CGC_ERR_ARG, "set_nlinks: bad arguments");
   const InstGeo& G = p.geo[inst];
@@ -586,7 +551,7 @@ static int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, cons
   return ok();
 }
 
-static cgc_options resolve_options(const cgc_options* o) {
+cgc_options resolve_options(const cgc_options* o) {
   cgc_options r{};
   r.struct_size = sizeof(cgc_options);
   r.local_pulses = 16;
@@ -638,7 +603,7 @@ static int host_bfs(Pool& p, uint32_t& id, int64_t& rounds) {
   return CGC_OK;
 }
 
-static int pool_solve(Pool& p, const cgc_options* opts) {
+int pool_solve(Pool& p, const cgc_options* opts) {
   const cgc_options o = resolve_options(opts);
   DevPool& d = p.dp;
   for (int i = 0; i < p.ninst; ++i) {
@@ -753,7 +718,7 @@ static int pool_solve(Pool& p, const cgc_options* opts) {
   return ok();
 }
 
-static int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host) {
+int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host) {
   if (inst < 0 || inst >= p.ninst || !out || (which != CGC_SEG_SINK_REACH && which != CGC_SEG_SOURCE_MIN))
     return fail(CGC_ERR_ARG, "get_segments: bad arguments");
   if (!p.solved) return fail(CGC_ERR_STATE, "get_segments: call maxflow first");
@@ -768,7 +733,7 @@ static int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mas
   return ok();
 }
 
-static int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess) {
+int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess) {
   if (inst < 0 || inst >= p.ninst) return fail(CGC_ERR_ARG, "get_residuals: bad instance");
   if (!p.solved) return fail(CGC_ERR_STATE, "get_residuals: call maxflow first");
   const InstGeo& G = p.geo[inst];
@@ -791,7 +756,7 @@ static int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* res
   return ok();
 }
 
-static int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count) {
+int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count) {
   if (!p.solved) return fail(CGC_ERR_STATE, "trace: call maxflow first");
   unsigned long long n = 0;
   CGC_CUDA(cudaMemcpy(&n, p.dp.stats + S_TRACE_N, 8, cudaMemcpyDeviceToHost));

@@ -149,7 +149,7 @@ struct ReachShared {
 //   tiles it pushed into for sweep id_next (persistent schedule); otherwise
 //   only the act[] flags are maintained (host-driven schedule).
 template <bool APPEND>
-__device__ void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
+__device__ inline void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
                            int32_t* sink_tiles = nullptr) {
@@ -307,7 +307,7 @@ __device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, in
   if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
 }
 
-__device__ void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
+__device__ inline void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
   const unsigned rm = __ldcg(P.rmask + g);
@@ -358,7 +358,7 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
 // until the tile is stable; re-queue face neighbours whose halo changed.
-__device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
+__device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
                          int32_t* list_next, int32_t* cnt_next) {
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
@@ -405,7 +405,7 @@ __device__ void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint
 // ---------------------------------------------------------------------------
 // Source-side reachability (canonical cut) after the maximum preflow:
 // closure of {v : e(v) > 0} over residual edges.
-__device__ void reach_init_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id0, int32_t* list0,
+__device__ inline void reach_init_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id0, int32_t* list0,
                                 int32_t* cnt0) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
@@ -427,7 +427,7 @@ __device__ void reach_init_tile(const DevPool& P, const int t, ReachShared& S, c
   __syncthreads();
 }
 
-__device__ void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
+__device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
                            int32_t* list_next, int32_t* cnt_next) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;

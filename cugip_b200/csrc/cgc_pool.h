@@ -1,0 +1,90 @@
+// Host-side pool of grid instances shared by the translation units of libcgc.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cgc.h"
+#include "cgc_device.cuh"
+#include "cgc_internal.h"
+
+namespace cgc {
+
+#define CGC_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::cgc::fail(e_ == cudaErrorMemoryAllocation ? CGC_ERR_OOM : CGC_ERR_CUDA,      \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+extern std::atomic<long long> g_launches;
+void note_launch();
+
+struct Pool {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int ninst = 0;
+  std::vector<InstGeo> geo;
+  std::vector<uint32_t> uploaded;  // bit 0 tlinks, bits 1..3 axes
+  int64_t maxN = 0;
+  int32_t T = 0;
+  int64_t Np = 0;
+  DevPool dp{};
+  void* dbuf = nullptr;          // all device state
+  int32_t* staging = nullptr;    // 2*maxN int32
+  uint8_t* seg = nullptr;        // maxN bytes
+  int32_t* pinned_cnt = nullptr; // host-pinned counters
+  bool solved = false;
+  int sms = 148;
+  int coop_blocks = 0;           // co-resident CTAs of k_solve
+  int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
+  int sweep_blocks = 0;
+  cgc_stats st{};
+  std::vector<int64_t> flows;
+  // device-resident batch path (cgc_batch_bind_* / cgc_batch_enqueue)
+  std::vector<const int32_t*> in_ptrs;   // 8 per instance: capS, capT, fwd[3], bwd[3]
+  std::vector<uint8_t*> out_ptrs;        // 2 per instance: source side, sink side
+  const int32_t** d_in = nullptr;        // device copy of in_ptrs
+  uint8_t** d_out = nullptr;             // device copy of out_ptrs
+  bool tables_dirty = true;
+  cudaStream_t cap_stream = nullptr;     // capture stream (the legacy stream cannot be captured)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_kernels = 0;                 // kernel nodes in the captured graph
+  ~Pool() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (dbuf) cudaFree(dbuf);
+    if (staging) cudaFree(staging);
+    if (seg) cudaFree(seg);
+    if (pinned_cnt) cudaFreeHost(pinned_cnt);
+  }
+};
+
+
+int check_device_error(Pool& p, const char* where);
+int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out);
+int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host);
+int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host);
+cgc_options resolve_options(const cgc_options* o);
+int pool_solve(Pool& p, const cgc_options* opts);
+int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host);
+int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess);
+int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count);
+// device-resident batch path (cgc_batch.cu)
+int pool_bind_inputs(Pool& p, int inst, const int32_t* capS, const int32_t* capT, const int32_t* const fwd[3],
+                     const int32_t* const bwd[3]);
+int pool_bind_outputs(Pool& p, int inst, uint8_t* source_side, uint8_t* sink_side);
+int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStream_t stream);
+int pool_wait(Pool& p, cudaStream_t stream);
+int pool_graph_create(Pool& p, const cgc_options* opts, int64_t* flows_dev);
+int pool_graph_launch(Pool& p);
+
+}  // namespace cgc

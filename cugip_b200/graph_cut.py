@@ -70,6 +70,33 @@ class Policy:
         return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
                             self.persistent, self.region_relabels, self.stall_sweeps, self.ctas_per_sm)
 
+    @classmethod
+    def from_options(cls, o: _lib.Options) -> "Policy":
+        return cls(local_pulses=o.local_pulses, sweeps_per_relabel=o.sweeps_per_relabel, schedule=o.schedule,
+                   max_sweeps=o.max_sweeps, persistent=o.persistent, region_relabels=o.region_relabels,
+                   stall_sweeps=o.stall_sweeps, ctas_per_sm=o.ctas_per_sm)
+
+    def __repr__(self):
+        return (f"Policy(L={self.local_pulses}, R={self.region_relabels}, K={self.sweeps_per_relabel}, "
+                f"ctas={self.ctas_per_sm}, stall={self.stall_sweeps})")
+
+
+def _autotune(fn, handle, candidates, repeats):
+    best = _lib.Options()
+    ms = C.c_double()
+    if candidates:
+        arr = (_lib.Options * len(candidates))(*[c.options() for c in candidates])
+        check(fn(handle, arr, len(candidates), repeats, C.byref(best), C.byref(ms)))
+    else:
+        check(fn(handle, None, 0, repeats, C.byref(best), C.byref(ms)))
+    return Policy.from_options(best), float(ms.value)
+
+
+def autotune_lookup(voxels: int, instances: int = 1) -> Policy | None:
+    o = _lib.Options()
+    rc = _lib.load().cgc_autotune_lookup(int(voxels), int(instances), C.byref(o))
+    return Policy.from_options(o) if rc == 0 else None
+
 
 class GridGraph:
     """X*Y*Z 6-connected grid graph; vertex id = x + X*(y + Y*z)."""
@@ -170,6 +197,10 @@ class GridGraph:
 
     def trace(self) -> list:
         return _read_trace(self._lib.cgc_grid_trace, self._h)
+
+    def autotune(self, candidates: list | None = None, repeats: int = 1):
+        """Fastest policy for the current capacities (which stay set): (policy, ms)."""
+        return _autotune(self._lib.cgc_grid_autotune, self._h, candidates, repeats)
 
 
 TRACE_KINDS = {1: "bfs_round", 2: "relabel_done", 3: "sweep", 4: "reach_round"}
@@ -306,3 +337,34 @@ class Batch:
 
     def trace(self) -> list:
         return _read_trace(self._lib.cgc_batch_trace, self._h)
+
+    # -- device-resident path (pointers to device memory, e.g. tensor.data_ptr())
+    def bind_inputs(self, i: int, cap_source_ptr: int, cap_sink_ptr: int, forward_ptrs, backward_ptrs=None) -> None:
+        f = (C.c_void_p * 3)(*[p or None for p in forward_ptrs])
+        b = None if backward_ptrs is None else (C.c_void_p * 3)(*[p or None for p in backward_ptrs])
+        check(self._lib.cgc_batch_bind_inputs(self._h, i, C.c_void_p(cap_source_ptr), C.c_void_p(cap_sink_ptr), f, b))
+
+    def bind_outputs(self, i: int, source_side_ptr: int | None, sink_side_ptr: int | None) -> None:
+        check(self._lib.cgc_batch_bind_outputs(self._h, i, C.c_void_p(source_side_ptr or 0),
+                                               C.c_void_p(sink_side_ptr or 0)))
+
+    def enqueue(self, policy: Policy | None = None, flows_ptr: int | None = None) -> None:
+        opts = policy.options() if policy else None
+        check(self._lib.cgc_batch_enqueue(self._h, C.byref(opts) if opts else None, C.c_void_p(flows_ptr or 0)))
+
+    def graph_create(self, policy: Policy | None = None, flows_ptr: int | None = None) -> None:
+        opts = policy.options() if policy else None
+        check(self._lib.cgc_batch_graph_create(self._h, C.byref(opts) if opts else None, C.c_void_p(flows_ptr or 0)))
+
+    def graph_launch(self) -> None:
+        check(self._lib.cgc_batch_graph_launch(self._h))
+
+    def autotune(self, candidates: list | None = None, repeats: int = 1):
+        """Fastest policy for the current capacities or bound inputs: (policy, ms)."""
+        return _autotune(self._lib.cgc_batch_autotune, self._h, candidates, repeats)
+
+    def wait(self) -> list[int]:
+        flows = np.zeros(len(self.extents), dtype=np.int64)
+        check(self._lib.cgc_batch_wait(self._h, flows.ctypes.data_as(_lib.P64)))
+        self.flows = [int(f) for f in flows]
+        return self.flows

@@ -208,6 +208,43 @@ int cgc_batch_set_nlinks(cgc_batch* b, int32_t i, int axis, const int32_t* fwd, 
 int cgc_batch_maxflow(cgc_batch* b, const cgc_options* opts, int64_t* flows /* count */);
 int cgc_batch_get_segments(cgc_batch* b, int32_t i, int which, uint8_t* out, uint8_t mask, uint8_t background);
 int cgc_batch_stats(cgc_batch* b, cgc_stats* out);
+
+/* Device-resident batches (no counterpart in the reference).  Bind each
+ * instance's device inputs once (capS, capT and the per-axis fwd/bwd n-link
+ * planes as in cgc_grid_set_nlinks; bwd may be NULL for symmetric n-links, a
+ * NULL axis is zero) and optional device outputs (X*Y*Z bytes of 1/0 for the
+ * minimal source side and the sink-reachable side).  The pointers are read
+ * again by every later solve, so new capacities are picked up by writing into
+ * the same buffers.  cgc_batch_enqueue queues one solve of every instance on
+ * the batch's stream without synchronising the host (flows_dev: device int64
+ * per instance, may be NULL); cgc_batch_graph_create captures that sequence
+ * once into a CUDA graph and cgc_batch_graph_launch replays it.
+ * cgc_batch_wait synchronises, returns the device status and copies the flows
+ * to the host (flows may be NULL). */
+int cgc_batch_bind_inputs(cgc_batch* b, int32_t i, const int32_t* capS, const int32_t* capT,
+                          const int32_t* const fwd[3], const int32_t* const bwd[3]);
+int cgc_batch_bind_outputs(cgc_batch* b, int32_t i, uint8_t* source_side, uint8_t* sink_side);
+int cgc_batch_enqueue(cgc_batch* b, const cgc_options* opts, int64_t* flows_dev);
+int cgc_batch_graph_create(cgc_batch* b, const cgc_options* opts, int64_t* flows_dev);
+int cgc_batch_graph_launch(cgc_batch* b);
+int cgc_batch_wait(cgc_batch* b, int64_t* flows);
+
+/* Autotuner (replaces the compile-time policies of
+ * detail/graph_cut_policies.hpp:23-89 with measured choices).  Times each
+ * candidate option set (n == 0: a built-in grid over local_pulses,
+ * region_relabels, sweeps_per_relabel and ctas_per_sm) `repeats` times on the
+ * grid's or batch's current capacities (set with the set_* calls, or bound
+ * device inputs), writes the fastest to *best (and its time in ms to
+ * *best_ms, either may be NULL) and caches it for the size class; the
+ * capacities are restored, so maxflow can follow directly.  With the
+ * environment variable CGC_AUTOTUNE_CACHE naming a file, results are appended
+ * to it and read back by cgc_autotune_lookup in later processes. */
+int cgc_grid_autotune(cgc_grid* g, const cgc_options* candidates, int32_t n, int32_t repeats,
+                      cgc_options* best, double* best_ms);
+int cgc_batch_autotune(cgc_batch* b, const cgc_options* candidates, int32_t n, int32_t repeats,
+                       cgc_options* best, double* best_ms);
+/* Cached options for a size class (total voxels, instance count); CGC_ERR_STATE if none. */
+int cgc_autotune_lookup(int64_t voxels, int32_t instances, cgc_options* out);
 int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count);
 
 /* ---- synthetic inputs ------------------------------------------------------

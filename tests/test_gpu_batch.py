@@ -1,0 +1,110 @@
+"""Device-resident batches (bound inputs/outputs, enqueue, CUDA graph replay)
+and the autotuner, checked against the golden fixtures."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cugip_b200 import volume
+from cugip_b200.graph_cut import SINK, SOURCE, Batch, GridGraph, Policy, autotune_lookup
+from tests.gpu_helpers import sha
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.json")))
+CASES = {(c["workload"], c["index"]): c for c in GOLDEN["cases"]}
+KEYS = [(4, i) for i in range(8)] + [(1, 0)]
+
+
+@pytest.fixture(scope="module")
+def device_batch():
+    import torch
+    vols = [volume.workload(*k) for k in KEYS]
+    dev = torch.device("cuda", 0)
+    ins = [[torch.from_numpy(a).to(dev) for a in v.arrays()] for v in vols]
+    outs = [(torch.zeros(v.N, dtype=torch.uint8, device=dev), torch.zeros(v.N, dtype=torch.uint8, device=dev))
+            for v in vols]
+    flows = torch.zeros(len(vols), dtype=torch.int64, device=dev)
+    B = Batch([(v.X, v.Y, v.Z) for v in vols])
+    for i, (d, o) in enumerate(zip(ins, outs)):
+        B.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
+        B.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
+    yield B, vols, ins, outs, flows
+    B.close()
+
+
+def _check(outs, flows_host):
+    for i, k in enumerate(KEYS):
+        c = CASES[k]
+        assert flows_host[i] == c["flow"], k
+        assert sha(outs[i][0].cpu().numpy()) == c["smin_sha256"], k
+        assert sha(outs[i][1].cpu().numpy()) == c["treach_sha256"], k
+
+
+def test_enqueue_matches_golden(device_batch):
+    B, vols, ins, outs, flows = device_batch
+    for o in outs:
+        o[0].fill_(7); o[1].fill_(7)
+    B.enqueue(Policy(), flows.data_ptr())
+    fl = B.wait()
+    assert fl == [int(x) for x in flows.cpu()]
+    _check(outs, fl)
+
+
+@pytest.mark.parametrize("policy", [Policy(), Policy(local_pulses=2, region_relabels=4, sweeps_per_relabel=4, ctas_per_sm=3)])
+def test_graph_replay_matches_golden(device_batch, policy):
+    B, vols, ins, outs, flows = device_batch
+    B.graph_create(policy, flows.data_ptr())
+    for rep in range(3):
+        for o in outs:
+            o[0].fill_(7); o[1].fill_(7)
+        flows.fill_(-1)
+        B.graph_launch()
+        fl = B.wait()
+        assert fl == [int(x) for x in flows.cpu()]
+        _check(outs, fl)
+
+
+def test_graph_picks_up_new_capacities(device_batch):
+    """The graph reads the bound buffers on every replay: overwrite instance 0
+    with all-zero capacities and its flow drops to 0."""
+    B, vols, ins, outs, flows = device_batch
+    B.graph_create(Policy(), flows.data_ptr())
+    saved = [t.clone() for t in ins[0]]
+    for t in ins[0]:
+        t.zero_()
+    B.graph_launch()
+    fl = B.wait()
+    assert fl[0] == 0 and fl[1:] == [CASES[k]["flow"] for k in KEYS[1:]]
+    for t, s in zip(ins[0], saved):
+        t.copy_(s)
+    B.graph_launch()
+    _check(outs, B.wait())
+
+
+def test_autotune_batch_and_lookup(device_batch):
+    B, vols, ins, outs, flows = device_batch
+    cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K) for L, R, K in
+             ((2, 4, 4), (4, 2, 8), (8, 1, 8))]
+    best, ms = B.autotune(cands, repeats=1)
+    assert ms > 0 and best.local_pulses in (2, 4, 8)
+    got = autotune_lookup(sum(v.N for v in vols), len(vols))
+    assert got is not None and got.local_pulses == best.local_pulses
+    B.enqueue(best, flows.data_ptr())
+    _check(outs, B.wait())
+
+
+def test_autotune_grid_keeps_capacities():
+    v = volume.workload(1)
+    g = GridGraph(v.X, v.Y, v.Z)
+    g.set_tweights(v.capS, v.capT)
+    for ax in range(3):
+        g.set_nweights(ax, v.n[ax])
+    best, ms = g.autotune(repeats=1)  # built-in candidate grid
+    assert ms > 0
+    c = CASES[(1, 0)]
+    assert g.max_flow(best) == c["flow"]
+    assert sha(g.fill_segments(mask=1, which=SOURCE)) == c["smin_sha256"]
+    assert sha(g.fill_segments(mask=1, which=SINK)) == c["treach_sha256"]
+    g.close()
