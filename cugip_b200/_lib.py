@@ -36,7 +36,8 @@ class Options(C.Structure):
     _fields_ = [("struct_size", C.c_int32), ("local_pulses", C.c_int32), ("sweeps_per_relabel", C.c_int32),
                 ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
                 ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("ctas_per_sm", C.c_int32), ("learned", C.c_int32), ("trace_cycles", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class Stats(C.Structure):
@@ -44,7 +45,7 @@ class Stats(C.Structure):
                 ("bfs_rounds", C.c_int64), ("tiles_swept", C.c_int64), ("tiles_relabelled", C.c_int64),
                 ("pulses", C.c_int64), ("solve_ms", C.c_double), ("kernel_ms", C.c_double),
                 ("launches", C.c_int64), ("bfs_ms", C.c_double), ("sweep_ms", C.c_double),
-                ("reach_ms", C.c_double), ("reserved", C.c_int64 * 3)]
+                ("reach_ms", C.c_double), ("sched_ms", C.c_double), ("reserved", C.c_int64 * 2)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -107,6 +108,15 @@ SIGNATURES = {
     "cgc_batch_autotune": (C.c_int, [VP, C.POINTER(Options), C.c_int32, C.c_int32, C.POINTER(Options),
                                      C.POINTER(C.c_double)]),
     "cgc_autotune_lookup": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(Options)]),
+    "cgc_scheduler_load": (C.c_int, [VP, VP]),
+    "cgc_scheduler_load_file": (C.c_int, [C.c_char_p]),
+    "cgc_grid_sched_trace": (C.c_int, [VP, VP, VP, VP, C.c_int32, P32]),
+    "cgc_trainer_create": (C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(VP)]),
+    "cgc_trainer_destroy": (C.c_int, [VP]),
+    "cgc_trainer_step": (C.c_int, [VP, C.c_int32, VP, VP, VP, VP, C.c_float, C.c_float, C.POINTER(C.c_float)]),
+    "cgc_trainer_eval": (C.c_int, [VP, C.c_int32, VP, VP, VP, VP, C.c_float, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float)]),
+    "cgc_trainer_weights": (C.c_int, [VP, VP, VP]),
     "cgc_volume_preset": (C.c_int, [C.c_int, C.c_int32, C.POINTER(VolumeSpec)]),
     "cgc_volume_generate": (C.c_int, [C.POINTER(VolumeSpec), VP, VP, VP, VP, VP, VP]),
 }
@@ -137,7 +147,8 @@ def check(rc: int) -> None:
 
 
 def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
-            persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0, ctas_per_sm: int = 0) -> Options:
+            persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0, ctas_per_sm: int = 0,
+            learned: int = 0, trace_cycles: int = 0) -> Options:
     o = Options()
     o.struct_size = C.sizeof(Options)
     o.local_pulses = local_pulses
@@ -148,4 +159,6 @@ def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 
     o.region_relabels = region_relabels
     o.stall_sweeps = stall_sweeps
     o.ctas_per_sm = ctas_per_sm
+    o.learned = learned
+    o.trace_cycles = trace_cycles
     return o

@@ -15,14 +15,15 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcgc.so")
 
-SOURCES = ["cgc_engine.cu", "cgc_batch.cu", "cgc_autotune.cu", "cgc_noalloc.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
-HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h"]
+SOURCES = ["cgc_engine.cu", "cgc_batch.cu", "cgc_autotune.cu", "cgc_sched_train.cu", "cgc_noalloc.cu",
+           "cgc_volume.cpp", "cgc_graph.cpp"]
+HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h", "cgc_sched.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-    "-shared",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-fopenmp",
+    "-shared", "-lgomp",
 ]
 
 

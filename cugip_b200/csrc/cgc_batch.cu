@@ -118,6 +118,10 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   for (int i = 0; i < p.ninst; ++i)
     if (!p.in_ptrs[8 * (size_t)i]) return fail(CGC_ERR_STATE, "enqueue: instance without bound inputs");
   const cgc_options o = resolve_options(opts);
+  if (o.learned > 0 || o.trace_cycles > 0) {  // buffers and weights before anything is queued
+    int rc = ensure_sched(p, o.learned > 0, o.trace_cycles);
+    if (rc) return rc;
+  }
   DevPool& d = p.dp;
   CGC_CUDA(cudaMemsetAsync(d.flow, 0, (size_t)p.ninst * 8, stream));
   CGC_CUDA(cudaMemsetAsync(d.stats, 0, S_NSTATS * 8, stream));
@@ -134,6 +138,8 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   prm.R = o.region_relabels;
   prm.K = o.sweeps_per_relabel;
   prm.stall = o.stall_sweeps;
+  prm.learned = o.learned;
+  prm.trace_cycles = o.trace_cycles;
   prm.max_sweeps = (int64_t)o.max_sweeps;
   prm.limit_ns = 20ull * 1000000000ull;
   const bool three = o.ctas_per_sm == 3;
@@ -183,6 +189,7 @@ int pool_wait(Pool& p, cudaStream_t stream) {
   p.st.bfs_ms = 1e-6 * (double)stats[S_NS_BFS];
   p.st.sweep_ms = 1e-6 * (double)stats[S_NS_SWEEP];
   p.st.reach_ms = 1e-6 * (double)stats[S_NS_REACH];
+  p.st.sched_ms = 1e-6 * (double)stats[S_NS_SCHED];
   return ok();
 }
 
@@ -190,6 +197,13 @@ int pool_graph_create(Pool& p, const cgc_options* opts, int64_t* flows_dev) {
   if (p.graph_exec) { cudaGraphExecDestroy(p.graph_exec); p.graph_exec = nullptr; }
   if (p.graph) { cudaGraphDestroy(p.graph); p.graph = nullptr; }
   if (!p.cap_stream) CGC_CUDA(cudaStreamCreateWithFlags(&p.cap_stream, cudaStreamNonBlocking));
+  {
+    const cgc_options o = resolve_options(opts);
+    if (o.learned > 0 || o.trace_cycles > 0) {  // allocations and weight uploads stay outside the capture
+      int rc = ensure_sched(p, o.learned > 0, o.trace_cycles);
+      if (rc) return rc;
+    }
+  }
   CGC_CUDA(cudaStreamBeginCapture(p.cap_stream, cudaStreamCaptureModeThreadLocal));
   const long long before = g_launches.load();
   int rc = pool_enqueue(p, opts, flows_dev, p.cap_stream);

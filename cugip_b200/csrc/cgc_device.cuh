@@ -20,6 +20,7 @@
 // engine keeps one out-residual plane per direction instead.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
 
 namespace cgc {
 
@@ -43,7 +44,7 @@ enum Counter {
 // statistics in DevPool::stats (unsigned long long)
 enum Stat {
   S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5,
-  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_NSTATS = 12
+  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_TRACE_CYC = 10, S_NS_SCHED = 11, S_NSTATS = 12
 };
 
 // phase trace records written by the persistent solve (two words each):
@@ -89,6 +90,19 @@ struct DevPool {
   int32_t* err;         // first error code raised on the device
   uint32_t* bar;        // grid barrier: [0] arrivals, [1] generation
   unsigned long long* trace;  // 2*TRACE_CAP words of phase records (may be null)
+  // learned scheduler (null unless used)
+  __nv_bfloat16* sfeat;       // T*16 tile features
+  __nv_bfloat16* sact0;       // T*16 activations of conv 1
+  __nv_bfloat16* sact1;       // T*16 activations of conv 2
+  const __nv_bfloat16* swconv;  // 3 layers * 27 taps * 16 * 16
+  const float* swhead;        // 2*16 weights + 2 biases
+  uint8_t* sbudget;           // T: pulses per visit until the next relabel
+  uint8_t* sprio;             // T: 1 = high priority
+  uint8_t* smask;             // T: region mask of the CNN stages (SchedMask bits)
+  // scheduling traces for training (null unless recorded)
+  __nv_bfloat16* tfeat;       // cycles*T*16 features at the start of each relabel cycle
+  uint8_t* tpulses;           // cycles*T: pulses of the tile's first visit in the cycle (0 = not visited)
+  uint8_t* tsink;             // cycles*T: 1 if the tile delivered flow to the sink during the cycle
 };
 
 __host__ __device__ inline int dir_axis(int d) { return d >> 1; }
@@ -99,6 +113,8 @@ struct SolveParams {
   int R;                 // region-relabel rounds per tile visit (0: pulses only)
   int K;                 // sweep pairs between global relabels
   int stall;             // relabel after this many sweeps without sink flow (0: never)
+  int learned;           // 1: budgets and priorities from the learned scheduler
+  int trace_cycles;      // record scheduling traces for the first trace_cycles relabel cycles
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
 };

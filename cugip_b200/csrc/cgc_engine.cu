@@ -23,6 +23,7 @@
 #include "cgc.h"
 #include "cgc_internal.h"
 #include "cgc_kernels.cuh"
+#include "cgc_sched.cuh"
 #include "cgc_pool.h"
 
 namespace cgc {
@@ -224,6 +225,7 @@ union SolveShared {
   SweepShared sw;
   BfsShared bfs;
   ReachShared rc;
+  SchedShared sched;
 };
 
 // The whole solve in one cooperative launch.
@@ -237,7 +239,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   int64_t s = 0;        // sweep index; sweep s uses list s&3 and stamp id s+1
   int64_t sweeps = 0;
   long long rounds = 0, relabels = 0;
-  unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0;
+  unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0, ns_sched = 0;
+  int traced = 0;
   uint64_t tmark = globaltimer_ns();
   const uint64_t t_launch = tmark;
   int ntrace = 0;
@@ -297,7 +300,68 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
       break;
     }
+    // ------------------------------------------------ learned scheduler
+    const int cycle = (int)relabels - 1;
+    const bool tracing = prm.trace_cycles > cycle;
+    if (tracing) traced = cycle + 1;
+    // The scheduler only pays off while active tiles outnumber the CTAs: with
+    // fewer, a sweep lasts one tile visit whatever the order or budgets.
+    const bool learned = prm.learned && nact > 2 * G;
+    if (learned || tracing) {
+      // stage 0: region mask (active tiles) and, when tracing, cleared trace rows
+      for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
+        P.smask[t] = __ldcg(P.act + t) ? (uint8_t)(SM_ACTIVE | SM_L3) : (uint8_t)0;
+        if (tracing) {
+          const int64_t r = (int64_t)cycle * P.T + t;
+          P.tpulses[r] = 0;
+          P.tsink[r] = 0;
+#pragma unroll
+          for (int c = 0; c < SCHED_C; ++c) P.tfeat[r * SCHED_C + c] = __float2bfloat16(0.f);
+        }
+      }
+      if (!grid_sync(P, prm.limit_ns)) return;
+      // stage 1: features of the active tiles (warp per tile), mask dilation
+      const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
+      for (int t = gw; t < P.T; t += nw) {
+        if (!(__ldcg(P.smask + t) & SM_ACTIVE)) continue;
+        sched_features_warp(P, t, P.sfeat);
+        if (tracing && (tid & 31) < SCHED_C) {
+          const int c = tid & 31;
+          P.tfeat[((int64_t)cycle * P.T + t) * SCHED_C + c] = P.sfeat[(int64_t)t * SCHED_C + c];
+        }
+      }
+      if (learned) {
+        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L3, SM_L2);
+        if (!grid_sync(P, prm.limit_ns)) return;
+        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L2, SM_L1);
+        if (!grid_sync(P, prm.limit_ns)) return;
+        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L1, SM_FEAT);
+        if (!grid_sync(P, prm.limit_ns)) return;
+        // inactive tiles that conv 1 reads hold zero features
+        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
+          const unsigned m = __ldcg(P.smask + t);
+          if ((m & SM_FEAT) && !(m & SM_ACTIVE)) {
+            uint4* f = reinterpret_cast<uint4*>(P.sfeat + (int64_t)t * SCHED_C);
+            f[0] = make_uint4(0, 0, 0, 0);
+            f[1] = make_uint4(0, 0, 0, 0);
+          }
+        }
+        if (!grid_sync(P, prm.limit_ns)) return;
+        for (int layer = 0; layer < 3; ++layer) {
+          sched_layer(P, layer, gw, nw);
+          if (!grid_sync(P, prm.limit_ns)) return;
+        }
+      } else if (!grid_sync(P, prm.limit_ns)) {
+        return;
+      }
+      lap(ns_sched);
+    }
     // ------------------------------------------------ sweeps
+    SweepExtra ex;
+    if (tracing) {
+      ex.tr_pulses = P.tpulses + (int64_t)cycle * P.T;
+      ex.tr_sink = P.tsink + (int64_t)cycle * P.T;
+    }
     int idle = 0;  // consecutive sweeps in which no tile delivered flow to the sink
     for (int j = 0; j < 2 * prm.K; ++j, ++s) {
       const int n = ld_cnt(sc + (s & 3));
@@ -306,9 +370,21 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
         sc[(s + 3) & 3] = 0;
         P.cnt[C_SINKT0 + (int)((s + 1) % 3)] = 0;
       }
-      for (int i = b; i < n; i += G)
-        sweep_tile<true>(P, __ldcg(sl[s & 3] + i), prm.L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), P.cnt + C_SINKT0 + (int)(s % 3));
+      ex.sink_tiles = P.cnt + C_SINKT0 + (int)(s % 3);
+      // the learned scheduler defers low-priority tiles during the first half
+      // of the cycle; every active tile is swept in the second half
+      const bool may_defer = learned && prm.learned == 1 && j < prm.K;
+      for (int i = b; i < n; i += G) {
+        const int t = __ldcg(sl[s & 3] + i);
+        if (may_defer && !__ldcg(P.sprio + t)) {
+          if (tid == 0 && atomicExch(P.stamp_sw + t, (uint32_t)(s + 3)) != (uint32_t)(s + 3))
+            sl[(s + 2) & 3][atomicAdd(sc + ((s + 2) & 3), 1)] = t;
+          continue;
+        }
+        const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
+        sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
+      }
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
       record(TR_SWEEP, sweeps, n);
@@ -346,6 +422,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     P.stats[S_NS_SWEEP] = ns_sweep;
     P.stats[S_NS_REACH] = ns_reach;
     P.stats[S_TRACE_N] = (unsigned long long)ntrace;
+    P.stats[S_TRACE_CYC] = (unsigned long long)traced;
+    P.stats[S_NS_SCHED] = ns_sched;
   }
 }
 
@@ -571,6 +649,8 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
     if (o->ctas_per_sm == 2 || o->ctas_per_sm == 3) r.ctas_per_sm = o->ctas_per_sm;
+    r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
+    r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
   return r;
 }
@@ -640,6 +720,12 @@ int pool_solve(Pool& p, const cgc_options* opts) {
     prm.R = o.region_relabels;
     prm.K = o.sweeps_per_relabel;
     prm.stall = o.stall_sweeps;
+    prm.learned = o.learned;
+    prm.trace_cycles = o.trace_cycles > 0 ? o.trace_cycles : 0;
+    if (prm.learned || prm.trace_cycles) {
+      rc = ensure_sched(p, prm.learned != 0, prm.trace_cycles);
+      if (rc) { destroy_events(); return rc; }
+    }
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
     void* args[] = {(void*)&d, (void*)&prm};
@@ -713,6 +799,7 @@ int pool_solve(Pool& p, const cgc_options* opts) {
   p.st.bfs_ms = 1e-6 * (double)stats[S_NS_BFS];
   p.st.sweep_ms = 1e-6 * (double)stats[S_NS_SWEEP];
   p.st.reach_ms = 1e-6 * (double)stats[S_NS_REACH];
+  p.st.sched_ms = 1e-6 * (double)stats[S_NS_SCHED];
   for (auto& u : p.uploaded) u = 0;
   p.solved = true;
   return ok();
@@ -851,6 +938,11 @@ int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count) {
 int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count) {
   if (!b || !count) return cgc::fail(CGC_ERR_ARG, "null argument");
   return cgc::pool_trace(*b->p, out, cap, count);
+}
+int cgc_grid_sched_trace(cgc_grid* g, uint16_t* feat, uint8_t* pulses, uint8_t* sink, int32_t max_cycles,
+                         int32_t* cycles) {
+  if (!g || !cycles) return cgc::fail(CGC_ERR_ARG, "null argument");
+  return cgc::pool_sched_trace(*g->p, feat, pulses, sink, max_cycles, cycles);
 }
 int cgc_grid_stats(cgc_grid* g, cgc_stats* out) {
   if (!g || !out) return cgc::fail(CGC_ERR_ARG, "null argument");

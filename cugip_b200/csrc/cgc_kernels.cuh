@@ -128,6 +128,7 @@ struct SweepShared {
   int out[2][6][TV];
   long long red[16];
   int flags;
+  int lastout;  // last pulse (1-based) that moved flow out of the tile or into the sink
 };
 
 struct BfsShared {
@@ -148,11 +149,18 @@ struct ReachShared {
 //   APPEND: queue the tile itself (if still active) for sweep id_self and the
 //   tiles it pushed into for sweep id_next (persistent schedule); otherwise
 //   only the act[] flags are maintained (host-driven schedule).
+// optional per-visit bookkeeping of the persistent schedule
+struct SweepExtra {
+  int32_t* sink_tiles = nullptr;  // counter of tiles that delivered sink flow in this sweep
+  uint8_t* tr_pulses = nullptr;   // trace: pulses of the first visit in this cycle
+  uint8_t* tr_sink = nullptr;     // trace: delivered sink flow in this cycle
+};
+
 template <bool APPEND>
 __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
-                           int32_t* sink_tiles = nullptr) {
+                           const SweepExtra ex = SweepExtra()) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -166,7 +174,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
   load_halo_heights(P, t, S.h);
   const int inst = __ldcg(P.tinst + t);
   const int hdead = P.geo[inst].hdead;
-  if (l == 0) S.flags = 0;
+  if (l == 0) { S.flags = 0; S.lastout = 0; }
   __syncthreads();
 
   int acc[6] = {0, 0, 0, 0, 0, 0};  // flow pushed out of the tile, per face
@@ -206,10 +214,12 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 #pragma unroll
       for (int d = 0; d < 6; ++d) hn[d] = S.h[cur][hi + hoff(d)];
       int pushed[6] = {0, 0, 0, 0, 0, 0};
+      bool moved_out = false;
       if (e > 0 && h < INF) {
         if (rT > 0 && h == 1) {
           const int dl = min(e, rT);
           e -= dl; rT -= dl; sink += dl;
+          moved_out = dl > 0;
         }
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
@@ -222,8 +232,9 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         if (inside(d, x, y, z)) S.out[cur][d][l] = pushed[d];
-        else acc[d] += pushed[d];
+        else { acc[d] += pushed[d]; moved_out = moved_out || pushed[d] > 0; }
       }
+      if (moved_out) S.lastout = pulses + 1;  // same value from every writer of this pulse
       __syncthreads();
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
@@ -280,8 +291,12 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
     P.act[t] = (uint8_t)(still ? 1 : 0);
     if (total) {
       atomicAdd(P.flow + inst, (unsigned long long)total);
-      if (sink_tiles) atomicAdd(sink_tiles, 1);
+      if (ex.sink_tiles) atomicAdd(ex.sink_tiles, 1);
+      if (ex.tr_sink) ex.tr_sink[t] = 1;
     }
+    // trace label: productive pulses of the tile's first visit in the cycle
+    // (255 marks a visited tile that moved nothing out)
+    if (ex.tr_pulses && ex.tr_pulses[t] == 0) ex.tr_pulses[t] = (uint8_t)(S.lastout > 0 ? min(S.lastout, 254) : 255);
     atomicAdd(P.stats + S_TILES_SWEPT, 1ull);
     atomicAdd(P.stats + S_PULSES, (unsigned long long)pulses);
     if (APPEND && still) {

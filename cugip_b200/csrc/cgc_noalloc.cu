@@ -193,6 +193,8 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   prm.R = o.region_relabels < 0 ? 0 : (o.region_relabels > 0 ? (o.region_relabels < 16 ? o.region_relabels : 16) : 1);
   prm.K = o.sweeps_per_relabel > 0 ? o.sweeps_per_relabel : 8;
   prm.stall = o.stall_sweeps > 0 ? o.stall_sweeps : 0;
+  prm.learned = 0;       // the learned scheduler needs allocated buffers
+  prm.trace_cycles = 0;
   prm.max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : (1 << 17);
   prm.limit_ns = 20ull * 1000000000ull;
   void* args[] = {(void*)&P, (void*)&prm};

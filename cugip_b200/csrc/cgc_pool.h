@@ -55,7 +55,14 @@ struct Pool {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_kernels = 0;                 // kernel nodes in the captured graph
+  // learned scheduler buffers (cgc_sched_train.cu)
+  void* sbuf = nullptr;
+  void* tbuf = nullptr;
+  int trace_cap = 0;
+  uint64_t sched_wver = 0;
   ~Pool() {
+    if (sbuf) cudaFree(sbuf);
+    if (tbuf) cudaFree(tbuf);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -86,5 +93,8 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
 int pool_wait(Pool& p, cudaStream_t stream);
 int pool_graph_create(Pool& p, const cgc_options* opts, int64_t* flows_dev);
 int pool_graph_launch(Pool& p);
+// learned scheduler (cgc_sched_train.cu)
+int ensure_sched(Pool& p, bool learned, int trace_cycles);
+int pool_sched_trace(Pool& p, uint16_t* feat, uint8_t* pulses, uint8_t* sink, int32_t max_cycles, int32_t* cycles);
 
 }  // namespace cgc

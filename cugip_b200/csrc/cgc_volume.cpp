@@ -74,6 +74,7 @@ void paint_soft_ball(std::vector<float>& img, const cgc_volume_spec& s, double c
   int64_t y0 = std::max<int64_t>(0, (int64_t)std::floor(cy - R)), y1 = std::min<int64_t>(s.Y - 1, (int64_t)std::ceil(cy + R));
   int64_t z0 = std::max<int64_t>(0, (int64_t)std::floor(cz - R)), z1 = std::min<int64_t>(s.Z - 1, (int64_t)std::ceil(cz + R));
   const double k = 1.0 / (std::sqrt(2.0) * sigma);
+#pragma omp parallel for schedule(static) if ((z1 - z0 + 1) * (y1 - y0 + 1) * (x1 - x0 + 1) > 65536)
   for (int64_t z = z0; z <= z1; ++z)
     for (int64_t y = y0; y <= y1; ++y)
       for (int64_t x = x0; x <= x1; ++x) {
@@ -204,12 +205,14 @@ extern "C" int cgc_volume_generate(const cgc_volume_spec* spec, int32_t* capS, i
   try { img.assign(size_t(N), float(s.background)); } catch (...) { return cgc::fail(CGC_ERR_OOM, "cgc_volume_generate: host allocation"); }
   Rng rng(s.seed);
   if (s.kind == 0) draw_spheres(img, s, rng); else draw_tubes(img, s, rng);
-  // noise, then likelihood t-links
+  // noise (one sequential stream, so the volume does not depend on the thread
+  // count), then likelihood t-links and contrast n-links in parallel
   std::vector<double> I((size_t)N);
+  for (int64_t v = 0; v < N; ++v) I[v] = double(img[v]) + s.noise_sd * rng.normal();
   const double inv2s2 = 1.0 / (2.0 * s.class_sd * s.class_sd);
+#pragma omp parallel for schedule(static)
   for (int64_t v = 0; v < N; ++v) {
-    double val = double(img[v]) + s.noise_sd * rng.normal();
-    I[v] = val;
+    const double val = I[v];
     if (image) image[v] = float(val);
     double a = ((val - s.mu_fg) * (val - s.mu_fg) - (val - s.mu_bg) * (val - s.mu_bg)) * inv2s2;
     double pfg = 1.0 / (1.0 + std::exp(a));
@@ -219,6 +222,7 @@ extern "C" int cgc_volume_generate(const cgc_volume_spec* spec, int32_t* capS, i
     capT[v] = round_cap(s.tlink_scale * -std::log(pfg));
   }
   const double ninv = 1.0 / (2.0 * s.nlink_sigma * s.nlink_sigma);
+#pragma omp parallel for schedule(static)
   for (int64_t z = 0; z < Z; ++z)
     for (int64_t y = 0; y < Y; ++y)
       for (int64_t x = 0; x < X; ++x) {

@@ -56,7 +56,9 @@ class Policy:
 
     def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0,
                  max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0,
-                 ctas_per_sm: int = 0):
+                 ctas_per_sm: int = 0, learned: int = 0, trace_cycles: int = 0):
+        self.learned = learned
+        self.trace_cycles = trace_cycles
         self.ctas_per_sm = ctas_per_sm
         self.region_relabels = region_relabels
         self.stall_sweeps = stall_sweeps
@@ -68,17 +70,25 @@ class Policy:
 
     def options(self) -> _lib.Options:
         return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
-                            self.persistent, self.region_relabels, self.stall_sweeps, self.ctas_per_sm)
+                            self.persistent, self.region_relabels, self.stall_sweeps, self.ctas_per_sm,
+                            self.learned, self.trace_cycles)
 
     @classmethod
     def from_options(cls, o: _lib.Options) -> "Policy":
         return cls(local_pulses=o.local_pulses, sweeps_per_relabel=o.sweeps_per_relabel, schedule=o.schedule,
                    max_sweeps=o.max_sweeps, persistent=o.persistent, region_relabels=o.region_relabels,
-                   stall_sweeps=o.stall_sweeps, ctas_per_sm=o.ctas_per_sm)
+                   stall_sweeps=o.stall_sweeps, ctas_per_sm=o.ctas_per_sm, learned=o.learned,
+                   trace_cycles=o.trace_cycles)
 
     def __repr__(self):
         return (f"Policy(L={self.local_pulses}, R={self.region_relabels}, K={self.sweeps_per_relabel}, "
-                f"ctas={self.ctas_per_sm}, stall={self.stall_sweeps})")
+                f"ctas={self.ctas_per_sm}, stall={self.stall_sweeps}, learned={self.learned})")
+
+    def with_(self, **kw) -> "Policy":
+        p = Policy.from_options(self.options())
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
 
 
 def _autotune(fn, handle, candidates, repeats):
@@ -197,6 +207,22 @@ class GridGraph:
 
     def trace(self) -> list:
         return _read_trace(self._lib.cgc_grid_trace, self._h)
+
+    def sched_trace(self, max_cycles: int = 64):
+        """Scheduling traces of the last solve (Policy.trace_cycles > 0): features
+        (cycles, T, 16) as uint16 BF16 bits, first-visit pulses (cycles, T) and
+        sink delivery (cycles, T)."""
+        n = C.c_int32()
+        check(self._lib.cgc_grid_sched_trace(self._h, None, None, None, 0, C.byref(n)))
+        c = min(n.value, max_cycles)
+        T = ((self.X + 7) // 8) * ((self.Y + 7) // 8) * ((self.Z + 7) // 8)
+        feat = np.zeros((c, T, 16), np.uint16)
+        pulses = np.zeros((c, T), np.uint8)
+        sink = np.zeros((c, T), np.uint8)
+        if c:
+            check(self._lib.cgc_grid_sched_trace(self._h, feat.ctypes.data, pulses.ctypes.data, sink.ctypes.data, c,
+                                                 C.byref(n)))
+        return feat, pulses, sink
 
     def autotune(self, candidates: list | None = None, repeats: int = 1):
         """Fastest policy for the current capacities (which stay set): (policy, ms)."""

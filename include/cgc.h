@@ -78,7 +78,9 @@ typedef struct cgc_options {
   int32_t region_relabels;    /* region-relabel rounds per tile visit (default 1, -1 = none) */
   int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
   int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers) or 3 (40 registers) */
-  int32_t reserved[7];
+  int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
+  int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
+  int32_t reserved[5];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */
@@ -96,7 +98,8 @@ typedef struct cgc_stats {
   double  bfs_ms;            /* persistent solve: time in exact global relabels */
   double  sweep_ms;          /* persistent solve: time in push sweeps */
   double  reach_ms;          /* persistent solve: time in the source-side reachability */
-  int64_t reserved[3];
+  double  sched_ms;          /* persistent solve: time in the learned scheduler (features + CNN) */
+  int64_t reserved[2];
 } cgc_stats;
 
 /* Kernels launched by this library on the calling process since load
@@ -245,6 +248,38 @@ int cgc_batch_autotune(cgc_batch* b, const cgc_options* candidates, int32_t n, i
                        cgc_options* best, double* best_ms);
 /* Cached options for a size class (total voxels, instance count); CGC_ERR_STATE if none. */
 int cgc_autotune_lookup(int64_t voxels, int32_t instances, cgc_options* out);
+
+/* ---- learned tile scheduler (no counterpart in the reference) -------------
+ * After every exact global relabel a small CNN over the tile grid (BF16
+ * weights and activations, FP32 accumulation; three 3x3x3 convolutions with
+ * 16 channels, then a linear head) reads per-tile features (log2 excess sum,
+ * active voxel count, 8-bin height histogram) and sets each tile's pulse
+ * budget (1..32) and priority; cgc_options.learned = 1 turns it on.  It only
+ * reorders pushes and relabels, so flows and cuts equal the plain solver's.
+ * Weights: 3*27*16*16 BF16 convolution weights ([layer][tap][cin][cout]) and
+ * 34 FP32 head values ([2][16] weights, then 2 biases); the file format is the
+ * 8-byte tag "CGCSCHD1" followed by both arrays. */
+int cgc_scheduler_load(const uint16_t* conv_bf16, const float* head);
+int cgc_scheduler_load_file(const char* path);
+/* Scheduling traces of the last solve run with cgc_options.trace_cycles > 0:
+ * for each recorded relabel cycle c and tile t (tile order of the grid,
+ * x fastest), feat[(c*T + t)*16 + k] (BF16 features), pulses[c*T + t] (pulses
+ * of the tile's first visit in the cycle, 0 = not visited) and sink[c*T + t]
+ * (1 if the tile delivered flow to the sink).  *cycles receives the number of
+ * recorded cycles; at most max_cycles are copied (host pointers, may be NULL). */
+int cgc_grid_sched_trace(cgc_grid* g, uint16_t* feat, uint8_t* pulses, uint8_t* sink, int32_t max_cycles,
+                         int32_t* cycles);
+/* Training kernels of the scheduler: Adam steps on device batches of feature
+ * grids (grids * D^3 * 16 BF16) with device float targets per tile (prio in
+ * {0,1}, budget in [0,1], mask 1 for tiles that count); count = sum of mask. */
+typedef struct cgc_trainer cgc_trainer;
+int cgc_trainer_create(int32_t max_grids, int32_t D, uint64_t seed, cgc_trainer** out);
+int cgc_trainer_destroy(cgc_trainer* t);
+int cgc_trainer_step(cgc_trainer* t, int32_t grids, const uint16_t* feat, const float* prio, const float* budget,
+                     const float* mask, float count, float lr, float* loss);
+int cgc_trainer_eval(cgc_trainer* t, int32_t grids, const uint16_t* feat, const float* prio, const float* budget,
+                     const float* mask, float count, float* loss, float* accuracy);
+int cgc_trainer_weights(cgc_trainer* t, uint16_t* conv_bf16, float* head);
 int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count);
 
 /* ---- synthetic inputs ------------------------------------------------------

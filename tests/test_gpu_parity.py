@@ -258,3 +258,57 @@ def test_snake_path_longer_than_a_tile():
     for pol in (None, Policy(persistent=-1), Policy(region_relabels=-1, local_pulses=2)):
         flow, smin, treach, _ = solve(X, Y, 1, capS.reshape(-1), capT.reshape(-1), fwd, None, pol)
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
+
+
+def _random_scheduler_weights(seed):
+    """Untrained (random) scheduler weights: the learned schedule must still be exact."""
+    import ctypes as C
+    lib = _lib.load()
+    h = C.c_void_p()
+    _lib.check(lib.cgc_trainer_create(1, 4, seed, C.byref(h)))
+    conv = np.zeros(3 * 27 * 256, np.uint16)
+    head = np.zeros(34, np.float32)
+    _lib.check(lib.cgc_trainer_weights(h, conv.ctypes.data, head.ctypes.data))
+    lib.cgc_trainer_destroy(h)
+    head[32:] = [0.0, 3.0]  # make budgets large and priorities mixed
+    _lib.check(lib.cgc_scheduler_load(conv.ctypes.data, head.ctypes.data))
+
+
+@pytest.mark.parametrize("learned", [1, 2])
+@pytest.mark.parametrize("key", [(1, 0), (4, 1), (2, 0)])
+def test_learned_scheduler_is_exact(key, learned):
+    """Budgets and priorities only reorder pushes and relabels: flow and both
+    cut sets stay bit-identical, with the committed weights and random ones."""
+    from cugip_b200 import scheduler
+    c = CASES[key]
+    v = volume.workload(*key)
+    for weights in ("committed", 7, 8):
+        if weights == "committed":
+            if not os.path.exists(scheduler.WEIGHTS):
+                continue
+            scheduler.load_weights()
+        else:
+            _random_scheduler_weights(weights)
+        for pol in (Policy(learned=learned), Policy(learned=learned, ctas_per_sm=3, local_pulses=2, region_relabels=4,
+                                                    sweeps_per_relabel=4)):
+            flow, smin, treach, st = solve(v.X, v.Y, v.Z, v.capS, v.capT, v.n, None, pol)
+            assert flow == c["flow"] and sha(smin) == c["smin_sha256"] and sha(treach) == c["treach_sha256"]
+
+
+def test_scheduling_traces_are_recorded():
+    from cugip_b200 import scheduler
+    v = volume.workload(5, 3)
+    g = GridGraph(v.X, v.Y, v.Z)
+    g.set_tweights(v.capS, v.capT)
+    for ax in range(3):
+        g.set_nweights(ax, v.n[ax])
+    g.max_flow(scheduler.TRACE_POLICY)
+    feat, pulses, sink = g.sched_trace()
+    g.close()
+    assert feat.shape[0] >= 1 and feat.shape[1] == 16 ** 3
+    import torch
+    f = torch.from_numpy(feat.astype(np.int16)).view(torch.bfloat16).float().numpy()
+    active = f[:, :, 1] > 0
+    assert active.any()
+    assert (pulses[active] > 0).all()          # every active tile was visited
+    assert not (f[~active] != 0).any()         # inactive tiles have zero features
