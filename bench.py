@@ -3,13 +3,21 @@
 
 A step is one full solve of the 256^3 forty-sphere workload (16.7 M voxels,
 50 M n-links, int32 capacities): capacities -> exact int64 flow, the minimal
-source set and the sink-reachable set.
+source set and the sink-reachable set, all checked against the oracle's
+golden answer after the timed region.
 
-  value : device-resident capacities (set_*_device), device-side masks;
-          whole-job voxels/s over all ranks (each rank solves its own replica:
-          a single grid does not shard, see DESIGN.md).
-  e2e   : the same through the host API (set_tweights/set_nweights from pinned
-          host arrays, masks copied back to the host), copies inside the timing.
+  value : the production path -- device-resident capacities bound to a
+          one-instance batch, the solve captured in a CUDA graph and replayed
+          once per step, masks written to device memory; the schedule is the
+          autotuner's choice among plain and learned-scheduler candidates.
+          Whole-job voxels/s over all ranks (each rank solves its own replica:
+          a single grid does not shard).
+  e2e   : the same step through the host API (GridGraph.set_tweights /
+          set_nweights from pinned host arrays, both masks copied back to the
+          host), copies inside the timing.
+  variants : plain fixed-schedule single solves vs tuned vs learned, on the
+          256^3 grid and on the 96-instance batch (extents 32..160): plain
+          sequential solves vs one batched graph launch vs learned + batched.
 
 `--impl reference` times the CPU max-flow path (the oracle's Boykov-Kolmogorov
 restatement of the reference's BK call site) on the host cores instead.
@@ -41,18 +49,17 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", type=int, default=2, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--local-pulses", type=int, default=0)
-    ap.add_argument("--sweeps-per-relabel", type=int, default=0)
-    ap.add_argument("--host-loop", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=96)
     return ap.parse_args()
 
 
-def golden_flow(workload: int):
+def golden(workload: int, index: int = 0):
     try:
         g = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
         for c in g["cases"]:
-            if c["workload"] == workload and c["index"] == 0:
-                return c["flow"]
+            if c["workload"] == workload and c["index"] == index:
+                return c
     except Exception:
         pass
     return None
@@ -91,14 +98,15 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+                                          "-lms", "100"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.2)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -150,6 +158,18 @@ def cpu_baseline(v, budget_s: float = 12.0, max_runs: int = 3):
             "seconds": med}
 
 
+_BK_CACHE = {}
+
+
+def _bk_worker(workload: int) -> float:
+    from cugip_b200 import volume
+    from oracle import oracle
+    if workload not in _BK_CACHE:
+        _BK_CACHE[workload] = volume.workload(workload)
+    v = _BK_CACHE[workload]
+    return oracle.maxflow_grid(v.X, v.Y, v.Z, v.capS, v.capT, v.n, algo=oracle.BK)[3]
+
+
 def run_reference(args, rank: int, world: int):
     """CPU reference arm: the oracle's BK port on the host cores (replicas of the
     workload solved concurrently by independent processes)."""
@@ -163,12 +183,10 @@ def run_reference(args, rank: int, world: int):
     times = []
     with ctx.Pool(procs) as pool:
         for it in range(args.warmup + args.steps):
-            t0 = time.time()
             secs = pool.map(_bk_worker, [args.workload] * procs)
-            wall = time.time() - t0
             if it >= args.warmup:
-                times.append((wall, max(secs)))
-    ms = 1000.0 * statistics.mean(t[1] for t in times)
+                times.append(max(secs))
+    ms = 1000.0 * statistics.mean(times)
     value = procs * v.N / (ms / 1000.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -181,18 +199,6 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
-_BK_CACHE = {}
-
-
-def _bk_worker(workload: int) -> float:
-    from cugip_b200 import volume
-    from oracle import oracle
-    if workload not in _BK_CACHE:
-        _BK_CACHE[workload] = volume.workload(workload)
-    v = _BK_CACHE[workload]
-    return oracle.maxflow_grid(v.X, v.Y, v.Z, v.capS, v.capT, v.n, algo=oracle.BK)[3]
-
-
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,61 +208,63 @@ def main():
         run_reference(args, rank, world)
         return
 
+    import hashlib
+    from datetime import timedelta
+
     import numpy as np
     import torch
     import torch.distributed as dist
-    from datetime import timedelta
 
-    from cugip_b200 import _lib, volume
-    from cugip_b200.graph_cut import SINK, SOURCE, GridGraph, Policy
+    from cugip_b200 import _lib, scheduler, volume
+    from cugip_b200.graph_cut import SINK, SOURCE, Batch, GridGraph, Policy
 
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     lib = _lib.load()
     _lib.check(lib.cgc_init(local))
+    have_learned = os.path.exists(scheduler.WEIGHTS)
+    if have_learned:
+        scheduler.load_weights()
 
-    v = volume.workload(args.workload)
-    N = v.N
-    want = golden_flow(args.workload)
-    dev = torch.device("cuda", local)
-    d_in = [torch.from_numpy(a).to(dev) for a in v.arrays()]          # capS, capT, nx, ny, nz
-    h_in = [torch.from_numpy(a).pin_memory() for a in v.arrays()]      # pinned host copies
-    d_seg = torch.empty((2, N), dtype=torch.uint8, device=dev)
-    h_seg = torch.empty((2, N), dtype=torch.uint8).pin_memory()
-    policy = Policy(local_pulses=args.local_pulses, sweeps_per_relabel=args.sweeps_per_relabel,
-                    persistent=-1 if args.host_loop else 0)
-    g = GridGraph(v.X, v.Y, v.Z)
-
-    def step_device():
-        g.set_tweights_device(d_in[0].data_ptr(), d_in[1].data_ptr())
-        for ax in range(3):
-            g.set_nweights_device(ax, d_in[2 + ax].data_ptr())
-        f = g.max_flow(policy)
-        g.fill_segments_device(d_seg[0].data_ptr(), 1, 0, SOURCE)
-        g.fill_segments_device(d_seg[1].data_ptr(), 1, 0, SINK)
-        return f
-
-    hn = [t.numpy() for t in h_in]
-    hs = [h_seg[0].numpy(), h_seg[1].numpy()]
-
-    def step_host():
-        g.set_tweights(hn[0], hn[1])
-        for ax in range(3):
-            g.set_nweights(ax, hn[2 + ax])
-        f = g.max_flow(policy)
-        g.fill_segments(hs[0], 1, 0, SOURCE)
-        g.fill_segments(hs[1], 1, 0, SINK)
-        return f
+    def sha(t):
+        return hashlib.sha256(np.ascontiguousarray(t).tobytes()).hexdigest()
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    dev = torch.device("cuda", local)
+    v = volume.workload(args.workload)
+    N = v.N
+    gold = golden(args.workload)
+    d_in = [torch.from_numpy(a).to(dev) for a in v.arrays()]          # capS, capT, nx, ny, nz
+    h_in = [torch.from_numpy(a).pin_memory() for a in v.arrays()]      # pinned host copies
+    d_seg = torch.zeros((2, N), dtype=torch.uint8, device=dev)
+    d_flow = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    # ---- production path: one-instance batch, bound device buffers, CUDA graph
+    B = Batch([(v.X, v.Y, v.Z)])
+    B.bind_inputs(0, d_in[0].data_ptr(), d_in[1].data_ptr(), [t.data_ptr() for t in d_in[2:]])
+    B.bind_outputs(0, d_seg[0].data_ptr(), d_seg[1].data_ptr())
+    cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr)
+             for (L, R, K) in ((4, 2, 8), (2, 4, 4), (8, 2, 8), (4, 2, 16), (2, 4, 8))
+             for c in (2, 3) for lr in ((0, 1) if have_learned else (0,))]
+    best, best_ms = B.autotune(cands, repeats=2)
+    B.graph_create(best, d_flow.data_ptr())
+
+    def check_outputs(flow):
+        if gold is None:
+            return
+        if flow != gold["flow"]:
+            raise SystemExit(f"flow {flow} differs from the oracle's {gold['flow']}")
+        if sha(d_seg[0].cpu().numpy()) != gold["smin_sha256"] or sha(d_seg[1].cpu().numpy()) != gold["treach_sha256"]:
+            raise SystemExit("cut sets differ from the oracle's")
+
     for _ in range(max(3, args.warmup)):
-        f = step_device()
-        if want is not None and f != want:
-            raise SystemExit(f"flow {f} differs from the oracle's {want}")
+        B.graph_launch()
+        check_outputs(B.wait()[0])
+    d_seg.zero_()
 
     uuid = None
     try:
@@ -264,8 +272,7 @@ def main():
     except Exception:
         pass
 
-    # ---- device-resident timing
-    stats = []
+    # ---- device-resident timing (graph replays)
     barrier()
     torch.cuda.synchronize()
     launches0 = lib.cgc_launch_count()
@@ -273,16 +280,33 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.steps):
-            step_device()
-            stats.append(g.stats())
+            B.graph_launch()
         e1.record()
         torch.cuda.synchronize()
     launches = lib.cgc_launch_count() - launches0
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clk.summary()
+    flow = B.wait()[0]
+    check_outputs(flow)
+    st = B.stats()
 
     # ---- end to end through the host API
+    g = GridGraph(v.X, v.Y, v.Z)
+    hn = [t.numpy() for t in h_in]
+    h_seg = torch.empty((2, N), dtype=torch.uint8).pin_memory()
+    hs = [h_seg[0].numpy(), h_seg[1].numpy()]
+
+    def step_host():
+        g.set_tweights(hn[0], hn[1])
+        for ax in range(3):
+            g.set_nweights(ax, hn[2 + ax])
+        f = g.max_flow(best)
+        g.fill_segments(hs[0], 1, 0, SOURCE)
+        g.fill_segments(hs[1], 1, 0, SINK)
+        return f
+
+    step_host()
     barrier()
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -293,51 +317,157 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms_e2e = e2.elapsed_time(e3) / args.steps
-    if want is not None and f != want:
-        raise SystemExit(f"flow {f} differs from the oracle's {want}")
-    if int(hs[0].sum()) == 0 and want:
-        raise SystemExit("empty source-side cut")
+    if gold and (f != gold["flow"] or sha(hs[0]) != gold["smin_sha256"] or sha(hs[1]) != gold["treach_sha256"]):
+        raise SystemExit("host-API result differs from the oracle's")
+
+    # k_solve alone: CUDA events around its launch on the grid's stream (cgc_stats.kernel_ms)
+    kms = []
+    for _ in range(3):
+        g.set_tweights_device(d_in[0].data_ptr(), d_in[1].data_ptr())
+        for ax in range(3):
+            g.set_nweights_device(ax, d_in[2 + ax].data_ptr())
+        g.max_flow(best)
+        kms.append(g.stats())
+    solve_ms = statistics.median(s["kernel_ms"] for s in kms)
 
     if world > 1:
         t = torch.tensor([ms, ms_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e = float(t[0]), float(t[1])
 
+    line = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
-        kms = statistics.mean(s["kernel_ms"] for s in stats)
-        swept = statistics.mean(s["tiles_swept"] for s in stats)
-        relabels = statistics.mean(s["global_relabels"] for s in stats)
+        swept = statistics.median(s["tiles_swept"] for s in kms)
+        relabels = statistics.median(s["global_relabels"] for s in kms)
         algo_bytes = 72.0 * 512.0 * swept + 36.0 * N * relabels
-        achieved = algo_bytes / (kms / 1000.0) / 1e9
-        traffic = profiled_traffic(args.workload)
+        achieved = algo_bytes / (solve_ms / 1000.0) / 1e9
         line = {
             "metric": METRIC, "value": world * N / (ms / 1000.0), "unit": "voxels/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload], "voxels": N, "n_links": int(
-                (v.X - 1) * v.Y * v.Z + v.X * (v.Y - 1) * v.Z + v.X * v.Y * (v.Z - 1)),
-                "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (capacities 335 MB, state 600 MB)",
-                "solver": "plain push-relabel, parity tile sweeps, persistent" if not args.host_loop else
-                          "plain push-relabel, host loop"},
+            "config": {"workload": WORKLOADS[args.workload], "voxels": N,
+                       "n_links": int((v.X - 1) * v.Y * v.Z + v.X * (v.Y - 1) * v.Z + v.X * v.Y * (v.Z - 1)),
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (capacities 335 MB, solver state 640 MB)",
+                       "path": "device-resident batch of 1, CUDA graph replay",
+                       "schedule": repr(best), "autotune_ms": best_ms},
             "e2e": {"value": world * N / (ms_e2e / 1000.0), "unit": "voxels/s",
                     "h2d_bytes_per_step": int(sum(a.nbytes for a in hn)), "d2h_bytes_per_step": int(2 * N)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "kernel": "k_solve", "kernel_ms": kms, "peak_source": peak_kind,
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
+                         "kernel": "k_solve", "kernel_ms": solve_ms, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes},
-            "solver_stats": {k: statistics.mean(s[k] for s in stats) for k in
-                             ("sweeps", "global_relabels", "bfs_rounds", "tiles_swept", "tiles_relabelled",
-                              "pulses", "solve_ms", "kernel_ms")},
-            "flow": int(f),
+            "solver_stats": {k: st[k] for k in ("sweeps", "global_relabels", "bfs_rounds", "tiles_swept",
+                                                "tiles_relabelled", "pulses", "bfs_ms", "sweep_ms", "reach_ms",
+                                                "sched_ms")},
+            "flow": int(flow),
             "clocks": clocks,
         }
+
+    # ---- variants: plain vs tuned vs learned, single grid and batch
+    if rank == 0 and world == 1 and not args.no_variants:
+        var = {}
+
+        def time_grid(pol, reps=5):
+            ts = []
+            for _ in range(reps):
+                g.set_tweights_device(d_in[0].data_ptr(), d_in[1].data_ptr())
+                for ax in range(3):
+                    g.set_nweights_device(ax, d_in[2 + ax].data_ptr())
+                e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0_.record()
+                fl = g.max_flow(pol)
+                g.fill_segments_device(d_seg[0].data_ptr(), 1, 0, SOURCE)
+                g.fill_segments_device(d_seg[1].data_ptr(), 1, 0, SINK)
+                e1_.record()
+                torch.cuda.synchronize()
+                ts.append(e0_.elapsed_time(e1_))
+                check_outputs(fl)
+            return statistics.median(ts)
+
+        plain_ms = time_grid(Policy())
+        var["grid_plain_default"] = {"ms": plain_ms, "voxels_per_s": N / plain_ms * 1e3, "schedule": repr(Policy())}
+        var["grid_production"] = {"ms": ms, "voxels_per_s": N / ms * 1e3, "schedule": repr(best)}
+        if have_learned:
+            lp = Policy.from_options(best.options())
+            lp.learned = 1
+            learned_ms = time_grid(lp)
+            var["grid_learned"] = {"ms": learned_ms, "voxels_per_s": N / learned_ms * 1e3, "schedule": repr(lp)}
+        var["grid_speedup_production_vs_plain"] = plain_ms / ms
+        # the 96-instance batched configuration
+        nb = args.batch_instances
+        vols = [volume.workload(4, i) for i in range(nb)]
+        tot = sum(x.N for x in vols)
+        dins = [[torch.from_numpy(a).to(dev) for a in x.arrays()] for x in vols]
+        douts = [torch.zeros((2, x.N), dtype=torch.uint8, device=dev) for x in vols]
+        # plain: one solve per instance through the single-grid API
+        seq = []
+        grids = [GridGraph(x.X, x.Y, x.Z) for x in vols]
+        for rep in range(2):
+            torch.cuda.synchronize()
+            e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0_.record()
+            for x, d, o, gg in zip(vols, dins, douts, grids):
+                gg.set_tweights_device(d[0].data_ptr(), d[1].data_ptr())
+                for ax in range(3):
+                    gg.set_nweights_device(ax, d[2 + ax].data_ptr())
+                gg.max_flow(Policy())
+                gg.fill_segments_device(o[0].data_ptr(), 1, 0, SOURCE)
+                gg.fill_segments_device(o[1].data_ptr(), 1, 0, SINK)
+            e1_.record()
+            torch.cuda.synchronize()
+            seq.append(e0_.elapsed_time(e1_))
+        seq_flows = [gg.flow for gg in grids]
+        for gg in grids:
+            gg.close()
+        seq_ms = min(seq)
+        BB = Batch([(x.X, x.Y, x.Z) for x in vols])
+        for i, (d, o) in enumerate(zip(dins, douts)):
+            BB.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
+            BB.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
+        bcands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c)
+                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4)) for c in (2, 3)]
+        bbest, _ = BB.autotune(bcands, repeats=1)
+
+        def time_batch(pol, reps=3):
+            BB.graph_create(pol)
+            ts = []
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0_.record()
+                BB.graph_launch()
+                e1_.record()
+                fl = BB.wait()
+                ts.append(e0_.elapsed_time(e1_))
+                if fl != seq_flows:
+                    raise SystemExit("batched flows differ from the single solves")
+            return statistics.median(ts)
+
+        bat_ms = time_batch(bbest)
+        var["batch96_plain_sequential"] = {"ms": seq_ms, "voxels_per_s": tot / seq_ms * 1e3, "schedule": repr(Policy())}
+        var["batch96_batched_graph"] = {"ms": bat_ms, "voxels_per_s": tot / bat_ms * 1e3, "schedule": repr(bbest)}
+        if have_learned:
+            lb = Policy.from_options(bbest.options())
+            lb.learned = 1
+            lbat_ms = time_batch(lb)
+            var["batch96_learned_batched"] = {"ms": lbat_ms, "voxels_per_s": tot / lbat_ms * 1e3,
+                                              "schedule": repr(lb)}
+            var["batch96_speedup_learned_batched_vs_plain"] = seq_ms / lbat_ms
+        var["batch96_speedup_batched_vs_plain"] = seq_ms / bat_ms
+        var["batch96_voxels"] = tot
+        BB.close()
+        line["variants"] = var
+
+    if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(v)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
     g.close()
+    B.close()
     if world > 1:
         dist.destroy_process_group()
 

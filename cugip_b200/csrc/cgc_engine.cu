@@ -632,12 +632,12 @@ int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32
 cgc_options resolve_options(const cgc_options* o) {
   cgc_options r{};
   r.struct_size = sizeof(cgc_options);
-  r.local_pulses = 16;
+  r.local_pulses = 4;
   r.sweeps_per_relabel = 8;
   r.schedule = CGC_SCHED_PARITY;
   r.max_sweeps = 1 << 17;
   r.persistent = 1;
-  r.region_relabels = 1;
+  r.region_relabels = 2;
   r.stall_sweeps = 0;
   r.ctas_per_sm = 2;
   if (o) {

@@ -189,8 +189,8 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   cgc_options o{};
   if (opts) o = *opts;
   SolveParams prm;
-  prm.L = o.local_pulses > 0 ? (o.local_pulses < 64 ? o.local_pulses : 64) : 16;
-  prm.R = o.region_relabels < 0 ? 0 : (o.region_relabels > 0 ? (o.region_relabels < 16 ? o.region_relabels : 16) : 1);
+  prm.L = o.local_pulses > 0 ? (o.local_pulses < 64 ? o.local_pulses : 64) : 4;
+  prm.R = o.region_relabels < 0 ? 0 : (o.region_relabels > 0 ? (o.region_relabels < 16 ? o.region_relabels : 16) : 2);
   prm.K = o.sweeps_per_relabel > 0 ? o.sweeps_per_relabel : 8;
   prm.stall = o.stall_sweeps > 0 ? o.stall_sweeps : 0;
   prm.learned = 0;       // the learned scheduler needs allocated buffers

@@ -70,12 +70,12 @@ enum {
    (include/cugip/advanced_operations/detail/graph_cut_policies.hpp:23-89). */
 typedef struct cgc_options {
   int32_t struct_size;
-  int32_t local_pulses;       /* push/relabel pulses per tile visit (1..64), default 16 */
+  int32_t local_pulses;       /* push/relabel pulses per region-relabel round (1..64), default 4 */
   int32_t sweeps_per_relabel; /* sweep pairs between global relabels, default 8 */
   int32_t schedule;           /* CGC_SCHED_* (default parity) */
   int32_t max_sweeps;         /* safety cap on sweeps, default 1<<17 */
   int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
-  int32_t region_relabels;    /* region-relabel rounds per tile visit (default 1, -1 = none) */
+  int32_t region_relabels;    /* region-relabel rounds per tile visit (default 2, -1 = none) */
   int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
   int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers) or 3 (40 registers) */
   int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
