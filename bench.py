@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=96)
+    ap.add_argument("--schedule", default="",
+                    help="fixed schedule L,R,K,ctas,learned (skips the autotuner; for profiling)")
     return ap.parse_args()
 
 
@@ -250,7 +252,11 @@ def main():
     cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr)
              for (L, R, K) in ((4, 2, 8), (2, 4, 4), (8, 2, 8), (4, 2, 16), (2, 4, 8))
              for c in (2, 3) for lr in ((0, 1) if have_learned else (0,))]
-    best, best_ms = B.autotune(cands, repeats=2)
+    if args.schedule:
+        L, R, K, c, lr = (int(x) for x in args.schedule.split(","))
+        best, best_ms = Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr), None
+    else:
+        best, best_ms = B.autotune(cands, repeats=2)
     B.graph_create(best, d_flow.data_ptr())
 
     def check_outputs(flow):
