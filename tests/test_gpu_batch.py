@@ -108,3 +108,11 @@ def test_autotune_grid_keeps_capacities():
     assert sha(g.fill_segments(mask=1, which=SOURCE)) == c["smin_sha256"]
     assert sha(g.fill_segments(mask=1, which=SINK)) == c["treach_sha256"]
     g.close()
+
+
+def test_sharded_solve_single_rank_matches_golden():
+    from cugip_b200.shard import solve_batch_on_rank, solve_sharded
+    keys = [(4, i) for i in range(5)]
+    vols = [volume.workload(*k) for k in keys]
+    flows = solve_sharded([(v.X, v.Y, v.Z) for v in vols], lambda idx: solve_batch_on_rank([vols[i] for i in idx]))
+    assert flows == [CASES[k]["flow"] for k in keys]
