@@ -117,6 +117,8 @@ SIGNATURES = {
     "cgc_trainer_eval": (C.c_int, [VP, C.c_int32, VP, VP, VP, VP, C.c_float, C.POINTER(C.c_float),
                                    C.POINTER(C.c_float)]),
     "cgc_trainer_weights": (C.c_int, [VP, VP, VP]),
+    "cgc_build_segmentation_graph": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, VP, VP, C.c_float, C.c_int32,
+                                               C.c_int32, C.c_int32, VP, VP, VP, VP, VP, VP]),
     "cgc_volume_preset": (C.c_int, [C.c_int, C.c_int32, C.POINTER(VolumeSpec)]),
     "cgc_volume_generate": (C.c_int, [C.POINTER(VolumeSpec), VP, VP, VP, VP, VP, VP]),
 }

@@ -16,7 +16,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcgc.so")
 
 SOURCES = ["cgc_engine.cu", "cgc_batch.cu", "cgc_autotune.cu", "cgc_sched_train.cu", "cgc_noalloc.cu",
-           "cgc_volume.cpp", "cgc_graph.cpp"]
+           "cgc_build.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
 HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h", "cgc_sched.cuh"]
 
 NVCC_FLAGS = [

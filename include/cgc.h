@@ -282,6 +282,22 @@ int cgc_trainer_eval(cgc_trainer* t, int32_t grids, const uint16_t* feat, const 
 int cgc_trainer_weights(cgc_trainer* t, uint16_t* conv_bf16, float* head);
 int cgc_batch_trace(cgc_batch* b, int64_t* out, int32_t cap, int32_t* count);
 
+/* ---- segmentation graph from an image and markers -------------------------
+ * Replaces the reference's host-side graph construction of its segmentation
+ * front-end (benchmarks/graph_cut/graph_cut.cpp:33-98): on the device, from a
+ * float image and a uint8 marker volume (x fastest, device pointers; markers
+ * may be NULL), writes int32 capacity volumes ready for the *_device setters:
+ * capS/capT = hard_tlink where the marker is 128 / 255, every voxel within 2
+ * voxels of the border is forced to the source (capS = hard_tlink, capT = 0),
+ * and the symmetric n-link to the +x/+y/+z neighbour (0 on the last slice) is
+ * round(nlink_scale * exp(-(Ii-Ij)^2 / 2 * sigma^2)) -- the reference's
+ * formula as written (graph_cut.cpp:73) -- or, with CGC_BUILD_GAUSSIAN,
+ * round(nlink_scale * exp(-(Ii-Ij)^2 / (2 sigma^2))).  Asynchronous on stream. */
+#define CGC_BUILD_GAUSSIAN 1
+int cgc_build_segmentation_graph(int32_t X, int32_t Y, int32_t Z, const float* image, const uint8_t* markers,
+                                 float sigma, int32_t nlink_scale, int32_t hard_tlink, int32_t flags,
+                                 int32_t* capS, int32_t* capT, int32_t* nx, int32_t* ny, int32_t* nz, void* stream);
+
 /* ---- synthetic inputs ------------------------------------------------------
  * Deterministic capacity volumes for the benchmark workloads (x-fastest,
  * int32): Gaussian spheres (a ball of radius r whose boundary is blurred by a
