@@ -142,20 +142,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   prm.trace_cycles = o.trace_cycles;
   prm.max_sweeps = (int64_t)o.max_sweeps;
   prm.limit_ns = 20ull * 1000000000ull;
-  const bool three = o.ctas_per_sm == 3;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(three ? p.coop_blocks3 : p.coop_blocks);
-  cfg.blockDim = dim3(512);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
-  else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
-  note_launch();
+  if (int rc = launch_solve(p, o, d, prm, stream)) return rc;
   bool any_out = false;
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;
   if (any_out) {

@@ -126,6 +126,8 @@ __global__ void k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __res
 __global__ void k_prepare(DevPool P);
 __global__ void k_solve(DevPool P, SolveParams prm);
 __global__ void k_solve3(DevPool P, SolveParams prm);
+constexpr int WARP_CTA_WARPS = 10;  // warps of the warp-per-tile solve CTA (one CTA per SM)
+__global__ void k_solve_w(DevPool P, SolveParams prm);
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);
 
 }  // namespace cgc

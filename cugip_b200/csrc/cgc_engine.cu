@@ -24,6 +24,7 @@
 #include "cgc_internal.h"
 #include "cgc_kernels.cuh"
 #include "cgc_sched.cuh"
+#include "cgc_warp.cuh"
 #include "cgc_pool.h"
 
 namespace cgc {
@@ -228,9 +229,18 @@ union SolveShared {
   SchedShared sched;
 };
 
-// The whole solve in one cooperative launch.
-__device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, SolveShared& S) {
+// The whole solve in one cooperative launch.  WARP = false: a CTA of 512
+// threads is the unit that visits a tile (SolveShared); WARP = true: every
+// warp of the CTA visits tiles on its own (WarpSmem per warp).
+template <bool WARP>
+__device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, void* smem) {
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  SolveShared& S = *reinterpret_cast<SolveShared*>(smem);
+  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem)[WARP ? (tid >> 5) : 0];
+  // tile-visiting units: CTAs or warps
+  const int U = WARP ? G * (int)(blockDim.x >> 5) : G;
+  const int u = WARP ? b * (int)(blockDim.x >> 5) + (tid >> 5) : b;
+  const bool leader = WARP ? (tid & 31) == 0 : tid == 0;
   int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
   int32_t* const sl[4] = {P.lists + 3 * P.T, P.lists + 4 * P.T, P.lists + 5 * P.T, P.lists + 6 * P.T};
   int32_t* const bc = P.cnt + C_BFS0;
@@ -265,7 +275,10 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
     }
     if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs);
+    for (int t = u; t < P.T; t += U) {
+      if constexpr (WARP) bfs_init_tile_w(P, t);
+      else bfs_init_tile(P, t, S.bfs);
+    }
     if (!grid_sync(P, prm.limit_ns)) return;
     for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x) bfs_queue_tile(P, t0 + tid, bfs_id, bl[0], bc + 0);
     if (!grid_sync(P, prm.limit_ns)) return;
@@ -274,7 +287,10 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const int n = ld_cnt(bc + k % 3);
       if (n == 0) break;
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-      for (int i = b; i < n; i += G) bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+      for (int i = u; i < n; i += U) {
+        if constexpr (WARP) bfs_tile_w(P, __ldcg(bl[k % 3] + i), W.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+        else bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+      }
       ++k;
       if (!grid_sync(P, prm.limit_ns)) return;
       record(TR_BFS_ROUND, rounds + k, n);
@@ -374,16 +390,20 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       // the learned scheduler defers low-priority tiles during the first half
       // of the cycle; every active tile is swept in the second half
       const bool may_defer = learned && prm.learned == 1 && j < prm.K;
-      for (int i = b; i < n; i += G) {
+      for (int i = u; i < n; i += U) {
         const int t = __ldcg(sl[s & 3] + i);
         if (may_defer && !__ldcg(P.sprio + t)) {
-          if (tid == 0 && atomicExch(P.stamp_sw + t, (uint32_t)(s + 3)) != (uint32_t)(s + 3))
+          if (leader && atomicExch(P.stamp_sw + t, (uint32_t)(s + 3)) != (uint32_t)(s + 3))
             sl[(s + 2) & 3][atomicAdd(sc + ((s + 2) & 3), 1)] = t;
           continue;
         }
         const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
-        sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
+        if constexpr (WARP)
+          sweep_tile_w<true>(P, t, L, prm.R, W.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+                             (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
+        else
+          sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+                           (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
       }
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
@@ -401,14 +421,20 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   // ------------------------------------------------ source-side reachability
   if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
   if (!grid_sync(P, prm.limit_ns)) return;
-  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, S.rc, bfs_id, bl[0], bc + 0);
+  for (int t = u; t < P.T; t += U) {
+    if constexpr (WARP) reach_init_tile_w(P, t, bfs_id, bl[0], bc + 0);
+    else reach_init_tile(P, t, S.rc, bfs_id, bl[0], bc + 0);
+  }
   if (!grid_sync(P, prm.limit_ns)) return;
   int k = 0;
   for (;;) {
     const int n = ld_cnt(bc + k % 3);
     if (n == 0) break;
     if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-    for (int i = b; i < n; i += G) reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+    for (int i = u; i < n; i += U) {
+      if constexpr (WARP) reach_tile_w(P, __ldcg(bl[k % 3] + i), W.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+      else reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+    }
     ++k;
     if (!grid_sync(P, prm.limit_ns)) return;
     record(TR_REACH_ROUND, k, n);
@@ -429,13 +455,44 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
 
 // The solve kernel at 2 CTAs per SM (64 registers) and at 3 (40 registers,
 // a few spills).
+int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.stream = stream;
+  if (o.warp_tiles) {
+    cfg.gridDim = dim3(p.coop_blocks_w);
+    cfg.blockDim = dim3(WARP_CTA_WARPS * 32);
+    cfg.dynamicSmemBytes = kWarpSmemBytes;
+    CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_w, d, prm));
+  } else {
+    const bool three = o.ctas_per_sm == 3;
+    cfg.gridDim = dim3(three ? p.coop_blocks3 : p.coop_blocks);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = 0;
+    if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
+    else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
+  }
+  note_launch();
+  return ok();
+}
+
 __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body(P, prm, S);
+  solve_body<false>(P, prm, &S);
 }
 __global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body(P, prm, S);
+  solve_body<false>(P, prm, &S);
+}
+// Warp per tile: one CTA of WARP_CTA_WARPS warps per SM, each warp with its
+// own WarpSmem slice of dynamic shared memory.
+__global__ void __launch_bounds__(WARP_CTA_WARPS * 32, 1) k_solve_w(DevPool P, SolveParams prm) {
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  solve_body<true>(P, prm, wsmem);
 }
 
 // Output kernels (linear layout of one instance).
@@ -582,6 +639,10 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   int occ3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_solve3, 512, 0));
   p->coop_blocks3 = std::max(1, occ3) * p->sms;
+  CGC_CUDA(cudaFuncSetAttribute(k_solve_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWarpSmemBytes));
+  int occw = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occw, k_solve_w, WARP_CTA_WARPS * 32, kWarpSmemBytes));
+  p->coop_blocks_w = std::max(1, occw) * p->sms;
   int occ2 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_sweep_list, 512, 0));
   p->sweep_blocks = std::max(1, occ2) * p->sms;
@@ -649,6 +710,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
     if (o->ctas_per_sm == 2 || o->ctas_per_sm == 3) r.ctas_per_sm = o->ctas_per_sm;
+    r.warp_tiles = o->warp_tiles > 0 ? 1 : 0;
     r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
@@ -728,12 +790,9 @@ int pool_solve(Pool& p, const cgc_options* opts) {
     }
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
-    void* args[] = {(void*)&d, (void*)&prm};
     CGC_CUDA(cudaEventRecord(evk0, p.stream));
-    const bool three = o.ctas_per_sm == 3;
-    CGC_CUDA(cudaLaunchCooperativeKernel(three ? (const void*)k_solve3 : (const void*)k_solve,
-                                         dim3(three ? p.coop_blocks3 : p.coop_blocks), dim3(512), args, 0, p.stream));
-    note_launch();
+    rc = launch_solve(p, o, d, prm, p.stream);
+    if (rc) { destroy_events(); return rc; }
     CGC_CUDA(cudaEventRecord(evk1, p.stream));
   } else {
     CGC_CUDA(cudaEventRecord(evk0, p.stream));

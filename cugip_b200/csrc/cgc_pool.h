@@ -42,6 +42,7 @@ struct Pool {
   int sms = 148;
   int coop_blocks = 0;           // co-resident CTAs of k_solve
   int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
+  int coop_blocks_w = 0;         // co-resident CTAs of k_solve_w
   int sweep_blocks = 0;
   cgc_stats st{};
   std::vector<int64_t> flows;
@@ -82,6 +83,8 @@ int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT,
 int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host);
 cgc_options resolve_options(const cgc_options* o);
 int pool_solve(Pool& p, const cgc_options* opts);
+// cooperative launch of the persistent solve kernel selected by the options
+int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream);
 int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host);
 int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess);
 int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count);

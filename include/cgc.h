@@ -80,7 +80,8 @@ typedef struct cgc_options {
   int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers) or 3 (40 registers) */
   int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
-  int32_t reserved[5];
+  int32_t warp_tiles;         /* persistent: 1 = one warp per tile visit (ten warps per SM), 0 = one 512-thread CTA */
+  int32_t reserved[4];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */
