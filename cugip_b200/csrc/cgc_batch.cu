@@ -142,6 +142,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   prm.trace_cycles = o.trace_cycles;
   prm.max_sweeps = (int64_t)o.max_sweeps;
   prm.limit_ns = 20ull * 1000000000ull;
+  prm.async = o.schedule == CGC_SCHED_ASYNC ? 1 : 0;
   if (int rc = launch_solve(p, o, d, prm, stream)) return rc;
   bool any_out = false;
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;

@@ -83,6 +83,12 @@ struct DevPool {
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
   uint32_t* stamp_sw;   // T: last sweep the tile was queued for
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
+  // work-queue schedule (null if unused): two queues (rings of qcap slots and
+  // their control blocks) and a lock word per tile (LOCK_W | readers)
+  int32_t* qring;       // 2*qcap
+  int32_t* qctl;        // 2*QCTL_INTS
+  int32_t qcap;
+  int32_t* tlock;       // T
   int32_t* cnt;         // C_NCOUNTERS
   unsigned long long* flow;   // ninst: flow value (int64 as two's complement)
   const InstGeo* geo;   // ninst
@@ -117,6 +123,7 @@ struct SolveParams {
   int trace_cycles;      // record scheduling traces for the first trace_cycles relabel cycles
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
+  int async = 0;         // 1: work-queue schedule (CGC_SCHED_ASYNC)
 };
 
 // kernels of cgc_engine.cu launched from other translation units
@@ -126,6 +133,8 @@ __global__ void k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __res
 __global__ void k_prepare(DevPool P);
 __global__ void k_solve(DevPool P, SolveParams prm);
 __global__ void k_solve3(DevPool P, SolveParams prm);
+__global__ void k_solve_q(DevPool P, SolveParams prm);
+__global__ void k_solve_q3(DevPool P, SolveParams prm);
 constexpr int WARP_CTA_WARPS = 10;  // warps of the warp-per-tile solve CTA (one CTA per SM)
 __global__ void k_solve_w(DevPool P, SolveParams prm);
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);

@@ -222,6 +222,58 @@ __device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
 __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }
 
 
+// Learned-scheduler stage at the start of a relabel cycle: region masks,
+// features, three convolution layers and the head (budgets and priorities
+// of the active tiles); with `tracing`, the features are also recorded.
+// Returns false when a barrier failed.
+__device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams& prm, int cycle, bool learned, bool tracing) {
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  // stage 0: region mask (active tiles) and, when tracing, cleared trace rows
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
+    P.smask[t] = __ldcg(P.act + t) ? (uint8_t)(SM_ACTIVE | SM_L3) : (uint8_t)0;
+    if (tracing) {
+      const int64_t r = (int64_t)cycle * P.T + t;
+      P.tpulses[r] = 0;
+      P.tsink[r] = 0;
+#pragma unroll
+      for (int c = 0; c < SCHED_C; ++c) P.tfeat[r * SCHED_C + c] = __float2bfloat16(0.f);
+    }
+  }
+  if (!grid_sync(P, prm.limit_ns)) return false;
+  // stage 1: features of the active tiles (warp per tile), mask dilation
+  const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
+  for (int t = gw; t < P.T; t += nw) {
+    if (!(__ldcg(P.smask + t) & SM_ACTIVE)) continue;
+    sched_features_warp(P, t, P.sfeat);
+    if (tracing && (tid & 31) < SCHED_C) {
+      const int c = tid & 31;
+      P.tfeat[((int64_t)cycle * P.T + t) * SCHED_C + c] = P.sfeat[(int64_t)t * SCHED_C + c];
+    }
+  }
+  if (!learned) return grid_sync(P, prm.limit_ns);
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L3, SM_L2);
+  if (!grid_sync(P, prm.limit_ns)) return false;
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L2, SM_L1);
+  if (!grid_sync(P, prm.limit_ns)) return false;
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L1, SM_FEAT);
+  if (!grid_sync(P, prm.limit_ns)) return false;
+  // inactive tiles that conv 1 reads hold zero features
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
+    const unsigned m = __ldcg(P.smask + t);
+    if ((m & SM_FEAT) && !(m & SM_ACTIVE)) {
+      uint4* f = reinterpret_cast<uint4*>(P.sfeat + (int64_t)t * SCHED_C);
+      f[0] = make_uint4(0, 0, 0, 0);
+      f[1] = make_uint4(0, 0, 0, 0);
+    }
+  }
+  if (!grid_sync(P, prm.limit_ns)) return false;
+  for (int layer = 0; layer < 3; ++layer) {
+    sched_layer(P, layer, gw, nw);
+    if (!grid_sync(P, prm.limit_ns)) return false;
+  }
+  return true;
+}
+
 union SolveShared {
   SweepShared sw;
   BfsShared bfs;
@@ -324,52 +376,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     // fewer, a sweep lasts one tile visit whatever the order or budgets.
     const bool learned = prm.learned && nact > 2 * G;
     if (learned || tracing) {
-      // stage 0: region mask (active tiles) and, when tracing, cleared trace rows
-      for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
-        P.smask[t] = __ldcg(P.act + t) ? (uint8_t)(SM_ACTIVE | SM_L3) : (uint8_t)0;
-        if (tracing) {
-          const int64_t r = (int64_t)cycle * P.T + t;
-          P.tpulses[r] = 0;
-          P.tsink[r] = 0;
-#pragma unroll
-          for (int c = 0; c < SCHED_C; ++c) P.tfeat[r * SCHED_C + c] = __float2bfloat16(0.f);
-        }
-      }
-      if (!grid_sync(P, prm.limit_ns)) return;
-      // stage 1: features of the active tiles (warp per tile), mask dilation
-      const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
-      for (int t = gw; t < P.T; t += nw) {
-        if (!(__ldcg(P.smask + t) & SM_ACTIVE)) continue;
-        sched_features_warp(P, t, P.sfeat);
-        if (tracing && (tid & 31) < SCHED_C) {
-          const int c = tid & 31;
-          P.tfeat[((int64_t)cycle * P.T + t) * SCHED_C + c] = P.sfeat[(int64_t)t * SCHED_C + c];
-        }
-      }
-      if (learned) {
-        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L3, SM_L2);
-        if (!grid_sync(P, prm.limit_ns)) return;
-        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L2, SM_L1);
-        if (!grid_sync(P, prm.limit_ns)) return;
-        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L1, SM_FEAT);
-        if (!grid_sync(P, prm.limit_ns)) return;
-        // inactive tiles that conv 1 reads hold zero features
-        for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
-          const unsigned m = __ldcg(P.smask + t);
-          if ((m & SM_FEAT) && !(m & SM_ACTIVE)) {
-            uint4* f = reinterpret_cast<uint4*>(P.sfeat + (int64_t)t * SCHED_C);
-            f[0] = make_uint4(0, 0, 0, 0);
-            f[1] = make_uint4(0, 0, 0, 0);
-          }
-        }
-        if (!grid_sync(P, prm.limit_ns)) return;
-        for (int layer = 0; layer < 3; ++layer) {
-          sched_layer(P, layer, gw, nw);
-          if (!grid_sync(P, prm.limit_ns)) return;
-        }
-      } else if (!grid_sync(P, prm.limit_ns)) {
-        return;
-      }
+      if (!sched_stage(P, prm, cycle, learned, tracing)) return;
       lap(ns_sched);
     }
     // ------------------------------------------------ sweeps
@@ -455,6 +462,170 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
 
 // The solve kernel at 2 CTAs per SM (64 registers) and at 3 (40 registers,
 // a few spills).
+// ---------------------------------------------------------------------------
+// The whole solve in one cooperative launch under the work-queue schedule
+// (CGC_SCHED_ASYNC).  A relabel cycle is: exact global relabel (BFS seeded
+// from the sink links, drained through the work queue), then push-relabel
+// visits of the active tiles through the work queue, with tile locks, until
+// the queue is empty or K visits per initially active tile were made.  The
+// phases of a cycle are separated by grid barriers; inside a phase no CTA
+// waits for another.  The end state is the one of the parity schedule: after
+// an exact relabel no tile holds an active vertex, so the preflow is maximum,
+// and the cut sets are computed from the final residual graph.
+__device__ __forceinline__ void solve_async(const DevPool& P, const SolveParams& prm, SolveShared& S) {
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  const int gtid = b * blockDim.x + tid, nthr = G * blockDim.x;
+  __shared__ int s_take;
+  // queue A: BFS and reachability; queue B: push-relabel visits
+  const WorkQueue qa{P.qring, P.qcap, P.qctl, prm.limit_ns};
+  const WorkQueue qb{P.qring + P.qcap, P.qcap, P.qctl + QCTL_INTS, prm.limit_ns};
+  uint32_t bfs_id = 1, sw_id = 1;
+  long long relabels = 0, cycles = 0;
+  unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0, ns_sched = 0;
+  int traced = 0;
+  uint64_t tmark = globaltimer_ns();
+  const uint64_t t_launch = tmark;
+  int ntrace = 0;
+  auto record = [&](unsigned long long kind, long long index, int tiles) {
+    if (b == 0 && tid == 0 && P.trace && ntrace < TRACE_CAP) {
+      P.trace[2 * ntrace] = (kind << 56) | ((unsigned long long)(index & 0xffffffffll) << 24) | (unsigned)(tiles & 0xffffff);
+      P.trace[2 * ntrace + 1] = globaltimer_ns() - t_launch;
+      ++ntrace;
+    }
+  };
+  auto lap = [&](unsigned long long& acc) {
+    const uint64_t now = globaltimer_ns();
+    acc += now - tmark;
+    tmark = now;
+  };
+  // both queues empty, no locks held (all CTAs, then a barrier)
+  auto reset_queues = [&]() {
+    for (int i = gtid; i < 2 * P.qcap; i += nthr) P.qring[i] = -1;
+    for (int i = gtid; i < P.T; i += nthr) P.tlock[i] = 0;
+    for (int i = gtid; i < 2 * QCTL_INTS; i += nthr) P.qctl[i] = 0;
+  };
+  // Visits tiles from queue q until the phase is over: q is drained (kind 0:
+  // BFS, 2: reachability) or, for push-relabel visits (kind 1), also once
+  // `budget` visits were made.
+  SweepExtra ex;
+  bool learned = false;
+  auto drain = [&](const WorkQueue& q, int kind, uint32_t id, int budget) {
+    if (ld_volatile(q.c(Q_PENDING)) == 0) return;  // nothing was queued
+    for (;;) {
+      if (tid == 0) {
+        int t = -1;  // -1: leave
+        const uint64_t t0 = globaltimer_ns();
+        for (;;) {
+          const int got = wq_take(q, P.err);
+          if (got == -2) raise_error(P, CGC_ERR_TIMEOUT);
+          if (got < 0) break;
+          if (kind != 1 || tile_try_lock(P, got)) {
+            atomicExch((kind == 1 ? P.stamp_sw : P.stamp_bfs) + got, 0u);  // may be queued again from now on
+            __threadfence();
+            t = got;
+            break;
+          }
+          // a face neighbour is being visited: back into the queue (its stamp
+          // is still set); this take is released after the new entry exists
+          if (!wq_push(q, got)) { raise_error(P, CGC_ERR_TIMEOUT); break; }
+          wq_release(q);
+          if (globaltimer_ns() - t0 > prm.limit_ns) { raise_error(P, CGC_ERR_TIMEOUT); break; }
+          __nanosleep(256);
+        }
+        s_take = t;
+      }
+      __syncthreads();
+      const int t = s_take;
+      __syncthreads();
+      if (t < 0) break;
+      if (kind == 0) {
+        bfs_tile(P, t, S.bfs, id, nullptr, nullptr, &q);
+      } else if (kind == 2) {
+        reach_tile(P, t, S.rc, id, nullptr, nullptr, &q);
+      } else {
+        const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
+        sweep_tile<true>(P, t, L, prm.R, S.sw, id, nullptr, nullptr, id, nullptr, nullptr, ex, &q);
+      }
+      if (tid == 0) {
+        if (kind == 1 && atomicAdd(q.c(Q_VISITS), 1) + 1 == budget) atomicExch(q.c(Q_DONE), 1);
+        wq_release(q);
+      }
+    }
+  };
+
+  for (;;) {
+    // ------------------------------------------------ exact global relabel
+    reset_queues();
+    if (!grid_sync(P, prm.limit_ns)) return;
+    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    ++bfs_id;
+    for (int t = gtid; t < P.T; t += nthr)
+      if (bfs_seed_tile(P, t)) enqueue(P, P.stamp_bfs, t, bfs_id, nullptr, nullptr, &qa);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    drain(qa, 0, bfs_id, 0);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    ++relabels;
+    record(TR_BFS_ROUND, relabels, 0);
+    lap(ns_bfs);
+    // ------------------------------------------------ active tiles -> queue B
+    ++sw_id;
+    for (int t = gtid; t < P.T; t += nthr)
+      if (__ldcg(P.act + t)) enqueue(P, P.stamp_sw, t, sw_id, nullptr, nullptr, &qb);
+    if (!grid_sync(P, prm.limit_ns)) return;
+    const int nact = ld_volatile(qb.c(Q_PENDING));
+    record(TR_RELABEL_DONE, relabels, nact);
+    if (nact == 0) break;
+    if ((cycles + 1) * 2 * (long long)prm.K > prm.max_sweeps) {
+      if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
+      break;
+    }
+    // ------------------------------------------------ learned scheduler
+    const int cycle = (int)relabels - 1;
+    const bool tracing = prm.trace_cycles > cycle;
+    if (tracing) traced = cycle + 1;
+    learned = prm.learned && nact > 2 * G;
+    if (learned || tracing) {
+      if (!sched_stage(P, prm, cycle, learned, tracing)) return;
+      lap(ns_sched);
+    }
+    // ------------------------------------------------ push-relabel visits
+    ex = SweepExtra();
+    if (tracing) {
+      ex.tr_pulses = P.tpulses + (int64_t)cycle * P.T;
+      ex.tr_sink = P.tsink + (int64_t)cycle * P.T;
+    }
+    const long long budget = (long long)prm.K * nact;
+    drain(qb, 1, sw_id, (int)(budget < (1ll << 30) ? budget : (1ll << 30)));
+    if (!grid_sync(P, prm.limit_ns)) return;
+    ++cycles;
+    record(TR_SWEEP, cycles, ld_volatile(qb.c(Q_VISITS)));
+    lap(ns_sweep);
+  }
+  lap(ns_bfs);
+  // ------------------------------------------------ source-side reachability
+  reset_queues();
+  if (!grid_sync(P, prm.limit_ns)) return;
+  ++bfs_id;
+  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, S.rc, bfs_id, nullptr, nullptr, &qa);
+  if (!grid_sync(P, prm.limit_ns)) return;
+  drain(qa, 2, bfs_id, 0);
+  if (!grid_sync(P, prm.limit_ns)) return;
+  record(TR_REACH_ROUND, 1, 0);
+  if (b == 0 && tid == 0) {
+    P.stats[S_SWEEPS] = (unsigned long long)cycles;
+    P.stats[S_RELABELS] = (unsigned long long)relabels;
+    P.stats[S_ROUNDS] = (unsigned long long)relabels;
+    lap(ns_reach);
+    P.stats[S_NS_BFS] = ns_bfs;
+    P.stats[S_NS_SWEEP] = ns_sweep;
+    P.stats[S_NS_REACH] = ns_reach;
+    P.stats[S_TRACE_N] = (unsigned long long)ntrace;
+    P.stats[S_TRACE_CYC] = (unsigned long long)traced;
+    P.stats[S_NS_SCHED] = ns_sched;
+  }
+}
+
 int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -463,7 +634,7 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cfg.stream = stream;
-  if (o.warp_tiles) {
+  if (o.warp_tiles && !prm.async) {
     cfg.gridDim = dim3(p.coop_blocks_w);
     cfg.blockDim = dim3(WARP_CTA_WARPS * 32);
     cfg.dynamicSmemBytes = kWarpSmemBytes;
@@ -473,8 +644,13 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
     cfg.gridDim = dim3(three ? p.coop_blocks3 : p.coop_blocks);
     cfg.blockDim = dim3(512);
     cfg.dynamicSmemBytes = 0;
-    if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
-    else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
+    if (prm.async) {
+      if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q3, d, prm));
+      else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q, d, prm));
+    } else {
+      if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
+      else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
+    }
   }
   note_launch();
   return ok();
@@ -487,6 +663,15 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
 __global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
   solve_body<false>(P, prm, &S);
+}
+// The solve under the work-queue schedule, at 2 and 3 CTAs per SM.
+__global__ void __launch_bounds__(512, 2) k_solve_q(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_async(P, prm, S);
+}
+__global__ void __launch_bounds__(512, 3) k_solve_q3(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_async(P, prm, S);
 }
 // Warp per tile: one CTA of WARP_CTA_WARPS warps per SM, each warp with its
 // own WarpSmem slice of dynamic shared memory.
@@ -581,6 +766,10 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   const int64_t o_sb = off; off += al(T * 4);
   const int64_t o_ss = off; off += al(T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
+  const int64_t o_lk = off; off += al(T * 4);
+  const int32_t qcap = queue_capacity((int32_t)T);
+  const int64_t o_qr = off; off += al(2 * (int64_t)qcap * 4);
+  const int64_t o_qc = off; off += al(2 * QCTL_INTS * 4);
   const int64_t o_cnt = off; off += al(C_NCOUNTERS * 4);
   const int64_t o_fl = off; off += al((int64_t)count * 8);
   const int64_t o_geo = off; off += al((int64_t)count * sizeof(InstGeo));
@@ -597,7 +786,8 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
   d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
   d.act = (uint8_t*)(base + o_act); d.tflag = (uint16_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
-  d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
+  d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt); d.tlock = (int32_t*)(base + o_lk);
+  d.qring = (int32_t*)(base + o_qr); d.qctl = (int32_t*)(base + o_qc); d.qcap = qcap;
   d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
   d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
   d.trace = (unsigned long long*)(base + o_tr);
@@ -639,6 +829,12 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   int occ3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_solve3, 512, 0));
   p->coop_blocks3 = std::max(1, occ3) * p->sms;
+  // the work-queue kernels have the same launch bounds; take the smaller grid
+  int occq = 0, occq3 = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, k_solve_q, 512, 0));
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq3, k_solve_q3, 512, 0));
+  p->coop_blocks = std::min(p->coop_blocks, std::max(1, occq) * p->sms);
+  p->coop_blocks3 = std::min(p->coop_blocks3, std::max(1, occq3) * p->sms);
   CGC_CUDA(cudaFuncSetAttribute(k_solve_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWarpSmemBytes));
   int occw = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occw, k_solve_w, WARP_CTA_WARPS * 32, kWarpSmemBytes));
@@ -790,6 +986,7 @@ int pool_solve(Pool& p, const cgc_options* opts) {
     }
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
+    prm.async = o.schedule == CGC_SCHED_ASYNC ? 1 : 0;
     CGC_CUDA(cudaEventRecord(evk0, p.stream));
     rc = launch_solve(p, o, d, prm, p.stream);
     if (rc) { destroy_events(); return rc; }

@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 #include "cgc.h"
 #include "cgc_device.cuh"
+#include "cgc_queue.cuh"
 
 namespace cgc {
 
@@ -105,6 +106,23 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t* li
   if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = item;
 }
 
+__device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
+                                           int32_t* cnt) {
+  if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
+}
+
+// queue_tile into the list of the next round, or into the work queue when one
+// is given (asynchronous schedule)
+__device__ __forceinline__ void enqueue(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
+                                        int32_t* cnt, const WorkQueue* wq) {
+  if (atomicExch(stamp + t, id) == id) return;
+  if (!wq) {
+    list[atomicAdd(cnt, 1)] = t;
+  } else if (!wq_push(*wq, t)) {
+    raise_error(P, CGC_ERR_TIMEOUT);
+  }
+}
+
 // block-wide int64 sum (512 threads); result valid in thread 0
 __device__ __forceinline__ long long block_sum64(long long v, long long* red) {
 #pragma unroll
@@ -160,7 +178,7 @@ template <bool APPEND>
 __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
-                           const SweepExtra ex = SweepExtra()) {
+                           const SweepExtra ex = SweepExtra(), const WorkQueue* wq = nullptr) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -299,16 +317,16 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
     if (ex.tr_pulses && ex.tr_pulses[t] == 0) ex.tr_pulses[t] = (uint8_t)(S.lastout > 0 ? min(S.lastout, 254) : 255);
     atomicAdd(P.stats + S_TILES_SWEPT, 1ull);
     atomicAdd(P.stats + S_PULSES, (unsigned long long)pulses);
-    if (APPEND && still) {
-      if (atomicExch(P.stamp_sw + t, id_self) != id_self) list_self[atomicAdd(cnt_self, 1)] = t;
-    }
+    // work queue: release the tile first, so that the tiles queued below can be
+    // locked as soon as they are taken
+    if (wq) tile_unlock(P, t);
   }
+  if (wq) __syncthreads();
+  if (APPEND && l == 0 && still) enqueue(P, P.stamp_sw, t, id_self, list_self, cnt_self, wq);
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
     P.act[nt] = 1;
-    if (APPEND) {
-      if (atomicExch(P.stamp_sw + nt, id_next) != id_next) list_next[atomicAdd(cnt_next, 1)] = nt;
-    }
+    if (APPEND) enqueue(P, P.stamp_sw, nt, id_next, list_next, cnt_next, wq);
   }
   __syncthreads();
 }
@@ -317,11 +335,6 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 // BFS seed for tile t: h = 1 where the sink residual is positive, INF elsewhere.
 // A tile with seeds is queued, and so is every face neighbour next to a seed
 // on the tile's face (the neighbour reads the seed through its halo).
-__device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
-                                           int32_t* cnt) {
-  if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
-}
-
 __device__ inline void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
@@ -353,8 +366,7 @@ __device__ inline void bfs_init_tile(const DevPool& P, const int t, BfsShared& S
 
 // Second BFS seeding step, one thread per tile: queue every tile that is not
 // all seeds and holds a seed or touches a seed on a neighbour's face.
-__device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0,
-                                               int32_t* cnt0) {
+__device__ __forceinline__ bool bfs_seed_tile(const DevPool& P, const int t) {
   bool q = false;
   if (t < P.T) {
     const int f = __ldcg(P.tflag + t);
@@ -366,15 +378,26 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
         if (nt >= 0 && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1)) q = true;  // dead tiles have no seed bits
       }
     }
-    if (q) P.stamp_bfs[t] = id0;
   }
+  return q;
+}
+
+__device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, const uint32_t id0, int32_t* list0,
+                                               int32_t* cnt0) {
+  const bool q = bfs_seed_tile(P, t);
+  if (q) P.stamp_bfs[t] = id0;
   warp_append(q, t, list0, cnt0);
 }
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
 // until the tile is stable; re-queue face neighbours whose halo changed.
+//
+// Work queue: a tile may be visited by two CTAs at once (it was queued again
+// while being visited).  Heights then only go down through atomicMin, and
+// the active flag is only ever set here (bfs_init_tile clears it): both
+// results are the ones of the visit that read the freshest halo.
 __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
-                         int32_t* list_next, int32_t* cnt_next) {
+                         int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
@@ -401,18 +424,19 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
     if (!any) break;
   }
   if (h < h0) {
-    P.h[g] = h;
+    const bool lowered = wq ? atomicMin(P.h + g, h) > h : true;
+    if (!wq) P.h[g] = h;
     const int fb = face_bits(x, y, z);
-    if (fb) atomicOr(&S.flags, fb);
+    if (fb && lowered) atomicOr(&S.flags, fb);
   }
   const int act = __syncthreads_or(has_excess && h < INF);
   if (l == 0) {
-    P.act[t] = (uint8_t)(act ? 1 : 0);
+    if (act) P.act[t] = 1;
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
   }
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id_next, list_next, cnt_next);
+    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id_next, list_next, cnt_next, wq);
   }
   __syncthreads();
 }
@@ -421,7 +445,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
 // Source-side reachability (canonical cut) after the maximum preflow:
 // closure of {v : e(v) > 0} over residual edges.
 __device__ inline void reach_init_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id0, int32_t* list0,
-                                int32_t* cnt0) {
+                                int32_t* cnt0, const WorkQueue* wq = nullptr) {
   const int l = threadIdx.x;
   const int64_t g = (int64_t)t * TV + l;
   const bool seed = (__ldcg(P.rmask + g) & 128u) != 0;
@@ -434,16 +458,16 @@ __device__ inline void reach_init_tile(const DevPool& P, const int t, ReachShare
   }
   __syncthreads();
   const int fl = S.flags;
-  if (l == 0 && (fl & 64)) queue_tile(P, P.stamp_bfs, t, id0, list0, cnt0);
+  if (l == 0 && (fl & 64)) enqueue(P, P.stamp_bfs, t, id0, list0, cnt0, wq);
   if (l < 6 && ((fl >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id0, list0, cnt0);
+    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id0, list0, cnt0, wq);
   }
   __syncthreads();
 }
 
 __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
-                           int32_t* list_next, int32_t* cnt_next) {
+                           int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -487,7 +511,7 @@ __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S,
   __syncthreads();
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id_next, list_next, cnt_next);
+    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id_next, list_next, cnt_next, wq);
   }
   __syncthreads();
 }

@@ -61,7 +61,9 @@ enum {
 /* schedules of the tile sweep */
 enum {
   CGC_SCHED_PARITY = 0, /* checkerboard tiles: halo heights exact, deterministic */
-  CGC_SCHED_ASYNC = 1   /* all active tiles each sweep, stale halo heights      */
+  CGC_SCHED_ASYNC = 1   /* work queue: tiles visited as soon as no face neighbour is
+                           being visited (tile locks), BFS label-correcting; no grid
+                           barrier per sweep or BFS round (persistent solve only) */
 };
 
 /* Solver options; zero-initialise and set struct_size = sizeof(cgc_options).

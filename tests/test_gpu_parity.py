@@ -34,6 +34,10 @@ POLICIES = {
     "warp_no_region": Policy(warp_tiles=1, region_relabels=-1, local_pulses=8),
     "warp_R3_L2": Policy(warp_tiles=1, local_pulses=2, region_relabels=3, sweeps_per_relabel=2),
     "warp_stall": Policy(warp_tiles=1, stall_sweeps=1, sweeps_per_relabel=64),
+    "async": Policy(schedule=1),
+    "async_L1_K1": Policy(schedule=1, local_pulses=1, sweeps_per_relabel=1),
+    "async_no_region": Policy(schedule=1, region_relabels=-1, local_pulses=8),
+    "async_cta3_R4": Policy(schedule=1, ctas_per_sm=3, local_pulses=2, region_relabels=4, sweeps_per_relabel=2),
 }
 
 
@@ -82,12 +86,12 @@ def test_long_paths_match_oracle(seed):
     for f in fwd + bwd:
         f[np.random.default_rng(seed).random(f.size) < 0.4] = 0
     f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
-    for pol in (None, Policy(persistent=-1), Policy(warp_tiles=1)):
+    for pol in (None, Policy(persistent=-1), Policy(warp_tiles=1), Policy(schedule=1)):
         flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, bwd, pol)
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "warp"])
+@pytest.mark.parametrize("policy", ["default", "warp", "async"])
 @pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 4, 5)])
 def test_golden_workloads(key, policy):
     c = CASES[key]
@@ -99,7 +103,7 @@ def test_golden_workloads(key, policy):
     assert sha(treach) == c["treach_sha256"]
 
 
-@pytest.mark.parametrize("policy", ["default", "warp"])
+@pytest.mark.parametrize("policy", ["default", "warp", "async"])
 @pytest.mark.parametrize("key", [(2, 0), (3, 0)])
 def test_full_size_workloads_with_certificate(key, policy):
     c = CASES[key]
@@ -195,7 +199,7 @@ def _face_case(X=16, Y=8, Z=8, sink_x=7, src_x=12, nlink=5):
     return X, Y, Z, capS.reshape(-1), capT.reshape(-1), [fx.reshape(-1), z, z]
 
 
-@pytest.mark.parametrize("policy", ["default", "host_loop", "warp"])
+@pytest.mark.parametrize("policy", ["default", "host_loop", "warp", "async"])
 @pytest.mark.parametrize("sink_x,src_x", [(7, 12), (8, 3), (7, 8), (0, 15)])
 def test_seeds_on_tile_faces(sink_x, src_x, policy):
     X, Y, Z, capS, capT, fwd = _face_case(sink_x=sink_x, src_x=src_x)
@@ -205,7 +209,7 @@ def test_seeds_on_tile_faces(sink_x, src_x, policy):
     assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "host_loop", "warp"])
+@pytest.mark.parametrize("policy", ["default", "host_loop", "warp", "async"])
 @pytest.mark.parametrize("seed", range(8))
 def test_sparse_terminals_match_oracle(seed, policy):
     """Very few t-links on a well connected grid: seeds land on tile faces and
@@ -217,7 +221,8 @@ def test_sparse_terminals_match_oracle(seed, policy):
     assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "host_loop", "no_region", "warp", "warp_no_region"])
+@pytest.mark.parametrize("policy", ["default", "host_loop", "no_region", "warp", "warp_no_region", "async",
+                                    "async_no_region"])
 @pytest.mark.parametrize("axis,n", [(0, 2), (0, 9), (0, 16), (0, 40), (1, 17), (2, 24), (0, 64)])
 def test_chain_through_every_voxel(axis, n, policy):
     """A 1-D chain with the source at one end and the sink at the other: the
@@ -263,7 +268,8 @@ def test_snake_path_longer_than_a_tile():
     f0, s0, t0, _ = oracle.maxflow_grid(X, Y, 1, capS.reshape(-1), capT.reshape(-1), fwd)
     assert f0 == 7
     for pol in (None, Policy(persistent=-1), Policy(region_relabels=-1, local_pulses=2), Policy(warp_tiles=1),
-                Policy(warp_tiles=1, region_relabels=-1, local_pulses=2)):
+                Policy(warp_tiles=1, region_relabels=-1, local_pulses=2), Policy(schedule=1),
+                Policy(schedule=1, region_relabels=-1, local_pulses=2)):
         flow, smin, treach, _ = solve(X, Y, 1, capS.reshape(-1), capT.reshape(-1), fwd, None, pol)
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
@@ -298,7 +304,8 @@ def test_learned_scheduler_is_exact(key, learned):
         else:
             _random_scheduler_weights(weights)
         for pol in (Policy(learned=learned), Policy(learned=learned, ctas_per_sm=3, local_pulses=2, region_relabels=4,
-                                                    sweeps_per_relabel=4), Policy(learned=learned, warp_tiles=1)):
+                                                    sweeps_per_relabel=4), Policy(learned=learned, warp_tiles=1),
+                    Policy(learned=learned, schedule=1)):
             flow, smin, treach, st = solve(v.X, v.Y, v.Z, v.capS, v.capT, v.n, None, pol)
             assert flow == c["flow"] and sha(smin) == c["smin_sha256"] and sha(treach) == c["treach_sha256"]
 
