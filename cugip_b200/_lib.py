@@ -79,6 +79,12 @@ SIGNATURES = {
     "cgc_grid_set_nlinks": (C.c_int, [VP, C.c_int, VP, VP]),
     "cgc_detect_grid": (C.c_int, [C.c_int32, C.c_int64, VP, VP, P32]),
     "cgc_grid_create_from_edges": (C.c_int, [C.c_int32, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(VP), P32]),
+    "cgc_graph_create": (C.c_int, [C.c_int32, C.c_int64, VP, VP, VP, VP, VP, C.POINTER(VP)]),
+    "cgc_graph_destroy": (C.c_int, [VP]),
+    "cgc_graph_set_tlinks": (C.c_int, [VP, VP, VP]),
+    "cgc_graph_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),
+    "cgc_graph_get_segments": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
+    "cgc_graph_stats": (C.c_int, [VP, C.POINTER(Stats)]),
     "cgc_grid_set_tlinks_device": (C.c_int, [VP, VP, VP]),
     "cgc_grid_set_nlinks_device": (C.c_int, [VP, C.c_int, VP, VP]),
     "cgc_grid_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),

@@ -25,6 +25,7 @@
 #include "cgc_kernels.cuh"
 #include "cgc_sched.cuh"
 #include "cgc_warp.cuh"
+#include "cgc_sync.cuh"
 #include "cgc_pool.h"
 
 namespace cgc {
@@ -192,31 +193,9 @@ __global__ void __launch_bounds__(512, 2) k_reach_round(DevPool P, const int32_t
 }
 
 // ---------------------------------------------------------------------------
-// Grid-wide barrier for the cooperative (co-resident) launch.  Waits are
-// bounded: after `limit_ns` the waiting CTA records CGC_ERR_TIMEOUT and every
-// CTA leaves the kernel at its next barrier.
+// Grid-wide barrier of the persistent solve (bounded waits, cgc_sync.cuh).
 __device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile uint32_t* gen = P.bar + 1;
-    const uint32_t g0 = *gen;
-    __threadfence();
-    const uint32_t arrived = atomicAdd(P.bar, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(P.bar, 0u);
-      __threadfence();
-      atomicAdd(P.bar + 1, 1u);
-    } else {
-      const uint64_t t0 = globaltimer_ns();
-      while (*gen == g0) {
-        __nanosleep(64);
-        if (globaltimer_ns() - t0 > limit_ns) { raise_error(P, CGC_ERR_TIMEOUT); break; }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *(volatile int32_t*)P.err == 0;
+  return grid_barrier(P.bar, P.err, limit_ns);
 }
 
 __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }

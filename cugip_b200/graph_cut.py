@@ -247,23 +247,89 @@ def _read_trace(fn, handle) -> list:
     return out
 
 
+class GenericGraph:
+    """Any edge list solved on the GPU (the non-grid path of cugip::Graph):
+    n vertices, edge i joins a[i] and b[i] with capacity cap_ab[i] from a[i]
+    to b[i] and cap_ba[i] back (cgc_graph_* in cgc.h)."""
+
+    def __init__(self, n: int, a, b, cap_ab, cap_ba, stream: int | None = None):
+        self._lib = _lib.load()
+        self.n = int(n)
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.int64).reshape(-1))
+        b = np.ascontiguousarray(np.asarray(b, dtype=np.int64).reshape(-1))
+        if a.size != b.size:
+            raise CgcError(1, "a and b must have the same length")
+        m = a.size
+        if m and (min(a.min(), b.min()) < 0 or max(a.max(), b.max()) >= self.n):
+            raise CgcError(1, "edge endpoints must lie in [0, n)")
+        a32, b32 = a.astype(np.int32), b.astype(np.int32)
+        f = _i32(cap_ab, m, "cap_ab")
+        w = _i32(cap_ba, m, "cap_ba")
+        h = C.c_void_p()
+        check(self._lib.cgc_graph_create(self.n, m, _ptr(a32), _ptr(b32), _ptr(f), _ptr(w), C.c_void_p(stream or 0),
+                                         C.byref(h)))
+        self._h = h
+        self.flow: int | None = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cgc_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_tweights(self, cap_source, cap_sink) -> None:
+        check(self._lib.cgc_graph_set_tlinks(self._h, _ptr(_i32(cap_source, self.n, "cap_source")),
+                                             _ptr(_i32(cap_sink, self.n, "cap_sink"))))
+
+    def max_flow(self, policy: Policy | None = None) -> int:
+        f = C.c_int64()
+        opts = policy.options() if policy is not None else None
+        check(self._lib.cgc_graph_maxflow(self._h, C.byref(opts) if opts is not None else None, C.byref(f)))
+        self.flow = int(f.value)
+        return self.flow
+
+    def fill_segments(self, out=None, mask: int = 255, background: int = 0, which: str = SINK):
+        seg = np.empty(self.n, np.uint8)
+        check(self._lib.cgc_graph_get_segments(self._h, _which(which), _ptr(seg), mask, background))
+        if out is None:
+            return seg
+        out[...] = seg.reshape(np.shape(out))
+        return out
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(self._lib.cgc_graph_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+
 class Graph:
     """Mirror of cugip::Graph<TFlow> (graph_cut.hpp:47-146) for int32 capacities.
 
     Edges are EdgeRecord(first, second) pairs with forward = cap first->second
-    and backward = cap second->first.  The edge list must describe a
-    6-connected grid with linear vertex ids (see cgc_grid_create_from_edges);
-    other graphs raise CgcError(CGC_ERR_NOT_GRID).
+    and backward = cap second->first.  An edge list that forms a 6-connected
+    grid with linear vertex ids (see cgc_grid_create_from_edges) goes to the
+    tile engine; any other graph goes to the generic CSR engine.
     """
 
     def __init__(self):
         self._n = 0
-        self._grid: GridGraph | None = None
+        self._solver: GridGraph | GenericGraph | None = None
         self._pending_t = None
 
     def set_vertex_count(self, count: int) -> None:
         self._n = int(count)
-        self._grid = None
+        self._solver = None
 
     def set_nweights(self, edge_count: int, edges, weights_forward, weights_backward) -> None:
         e = np.ascontiguousarray(np.asarray(edges, dtype=np.int64).reshape(-1, 2)[:edge_count])
@@ -274,37 +340,49 @@ class Graph:
         h = C.c_void_p()
         dims = (C.c_int32 * 3)()
         lib = _lib.load()
-        check(lib.cgc_grid_create_from_edges(self._n, edge_count, _ptr(a), _ptr(b), _ptr(f), _ptr(w),
-                                             None, C.byref(h), dims))
-        self._grid = GridGraph._wrap(h, list(dims))
+        rc = lib.cgc_grid_create_from_edges(self._n, edge_count, _ptr(a), _ptr(b), _ptr(f), _ptr(w),
+                                            None, C.byref(h), dims)
+        if rc == 8:  # CGC_ERR_NOT_GRID: the generic engine takes it
+            self._solver = GenericGraph(self._n, e[:, 0], e[:, 1], f, w)
+        else:
+            check(rc)
+            self._solver = GridGraph._wrap(h, list(dims))
         if self._pending_t is not None:
-            self._grid.set_tweights(*self._pending_t)
-            self._pending_t = None
+            self._solver.set_tweights(*self._pending_t)
 
     def set_tweights(self, cap_source, cap_sink) -> None:
-        if self._grid is None:
-            # the reference allows t-links before n-links; keep them until the grid exists
-            self._pending_t = (_i32(cap_source, self._n, "cap_source"), _i32(cap_sink, self._n, "cap_sink"))
-            return
-        self._grid.set_tweights(cap_source, cap_sink)
+        # the reference accepts t-links before n-links; keep them for the graph
+        # set_nweights builds next
+        self._pending_t = (_i32(cap_source, self._n, "cap_source"), _i32(cap_sink, self._n, "cap_sink"))
+        if self._solver is not None:
+            self._solver.set_tweights(*self._pending_t)
 
     def max_flow(self, policy: Policy | None = None) -> int:
-        if self._grid is None:
+        if self._solver is None:
             raise CgcError(7, "max_flow: set_nweights was not called")
-        return self._grid.max_flow(policy)
+        return self._solver.max_flow(policy)
 
     def fill_segments(self, out=None, mask: int = 255, background: int = 0, which: str = SINK):
-        if self._grid is None:
+        if self._solver is None:
             raise CgcError(7, "fill_segments: no graph")
-        seg = self._grid.fill_segments(None, mask, background, which)
+        seg = self._solver.fill_segments(None, mask, background, which)
         if out is None:
             return seg
         out[...] = seg.reshape(np.shape(out))
         return out
 
+    def stats(self) -> dict:
+        if self._solver is None:
+            raise CgcError(7, "stats: no graph")
+        return self._solver.stats()
+
     @property
     def grid(self) -> GridGraph | None:
-        return self._grid
+        return self._solver if isinstance(self._solver, GridGraph) else None
+
+    @property
+    def generic(self) -> GenericGraph | None:
+        return self._solver if isinstance(self._solver, GenericGraph) else None
 
 
 class Batch:

@@ -148,6 +148,24 @@ int cgc_grid_create_from_edges(int32_t n, int64_t m, const uint32_t* a, const ui
                                const int32_t* fwd, const int32_t* bwd, void* stream, cgc_grid** out,
                                int32_t* dims_out);
 
+/* ---- generic graphs ----------------------------------------------------------
+ * Any edge list (the non-grid path of Graph::set_vertex_count / set_nweights /
+ * set_tweights / max_flow / fill_segments, graph_cut.hpp:213-333): n vertices,
+ * edge i joins a[i] and b[i] with capacity cap_ab[i] from a[i] to b[i] and
+ * cap_ba[i] back (EdgeRecord(first, second) with the forward and backward
+ * weights).  Self loops are ignored, parallel edges are separate arcs.  The
+ * residual graph is built on the device (CSR); arrays are host memory and are
+ * copied.  The options' sweeps_per_relabel sets the pulses between exact
+ * relabels (2x) and max_sweeps caps the pulses.  Cut semantics as for grids. */
+typedef struct cgc_graph cgc_graph;
+int cgc_graph_create(int32_t n, int64_t m, const int32_t* a, const int32_t* b, const int32_t* cap_ab,
+                     const int32_t* cap_ba, void* stream, cgc_graph** out);
+int cgc_graph_destroy(cgc_graph* g);
+int cgc_graph_set_tlinks(cgc_graph* g, const int32_t* capS, const int32_t* capT);
+int cgc_graph_maxflow(cgc_graph* g, const cgc_options* opts, int64_t* flow);
+int cgc_graph_get_segments(cgc_graph* g, int which, uint8_t* out, uint8_t mask, uint8_t background);
+int cgc_graph_stats(cgc_graph* g, cgc_stats* stats);
+
 /* Same as the two setters above with device pointers (no host copies). */
 int cgc_grid_set_tlinks_device(cgc_grid* g, const int32_t* capS, const int32_t* capT);
 int cgc_grid_set_nlinks_device(cgc_grid* g, int axis, const int32_t* fwd, const int32_t* bwd);

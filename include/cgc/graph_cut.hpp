@@ -129,10 +129,44 @@ class GridGraph {
   int X_, Y_, Z_;
 };
 
-// Drop-in for cugip::Graph<TFlow> (graph_cut.hpp:47-146).  The edge list must
-// form a 6-connected grid with linear vertex ids; other graphs throw
-// Exception(CGC_ERR_NOT_GRID).  Unlike the reference, the graph can be solved
-// again after setting new weights.
+// Any edge list on the GPU (cgc_graph_*): the non-grid path of Graph.
+class GenericGraph {
+ public:
+  GenericGraph(int32_t n, int64_t m, const int32_t* a, const int32_t* b, const int32_t* cap_ab, const int32_t* cap_ba)
+      : n_(n) {
+    check(cgc_graph_create(n, m, a, b, cap_ab, cap_ba, nullptr, &g_), "set_nweights");
+  }
+  GenericGraph(const GenericGraph&) = delete;
+  GenericGraph& operator=(const GenericGraph&) = delete;
+  ~GenericGraph() { if (g_) cgc_graph_destroy(g_); }
+
+  size_t size() const { return (size_t)n_; }
+  void set_tweights(const int32_t* capS, const int32_t* capT) { check(cgc_graph_set_tlinks(g_, capS, capT), "set_tweights"); }
+  int64_t max_flow(const GraphCutPolicy* policy = nullptr) {
+    int64_t f = 0;
+    cgc_options o;
+    if (policy) o = policy->options();
+    check(cgc_graph_maxflow(g_, policy ? &o : nullptr, &f), "max_flow");
+    return f;
+  }
+  void segments(int which, uint8_t* out, uint8_t mask = 255, uint8_t bg = 0) const {
+    check(cgc_graph_get_segments(g_, which, out, mask, bg), "fill_segments");
+  }
+  cgc_stats stats() const {
+    cgc_stats s;
+    check(cgc_graph_stats(g_, &s), "stats");
+    return s;
+  }
+
+ private:
+  cgc_graph* g_ = nullptr;
+  int32_t n_;
+};
+
+// Drop-in for cugip::Graph<TFlow> (graph_cut.hpp:47-146).  An edge list that
+// forms a 6-connected grid with linear vertex ids goes to the tile engine,
+// any other graph to the generic engine.  Unlike the reference, the graph can
+// be solved again after setting new weights.
 template <typename TFlow>
 class Graph {
  public:
@@ -142,6 +176,7 @@ class Graph {
   void set_vertex_count(int count) {
     n_ = count;
     grid_.reset();
+    generic_.reset();
     tlink_s_.clear();
     tlink_t_.clear();
   }
@@ -153,18 +188,25 @@ class Graph {
     std::vector<int32_t> w = detail::to_i32(bwd, edge_count, "set_nweights");
     cgc_grid* g = nullptr;
     int32_t dims[3];
-    check(cgc_grid_create_from_edges(n_, edge_count, a.data(), b.data(), f.data(), w.data(), nullptr, &g, dims),
-          "set_nweights");
-    grid_.reset(new GridGraph(g, dims[0], dims[1], dims[2]));
+    grid_.reset();
+    generic_.reset();
+    const int rc = cgc_grid_create_from_edges(n_, edge_count, a.data(), b.data(), f.data(), w.data(), nullptr, &g, dims);
+    if (rc == CGC_ERR_NOT_GRID) {
+      std::vector<int32_t> ai(a.begin(), a.end()), bi(b.begin(), b.end());
+      generic_.reset(new GenericGraph(n_, edge_count, ai.data(), bi.data(), f.data(), w.data()));
+    } else {
+      check(rc, "set_nweights");
+      grid_.reset(new GridGraph(g, dims[0], dims[1], dims[2]));
+    }
     // t-links set earlier (the reference accepts them in either order) apply
-    // to the new grid as well
-    if (!tlink_s_.empty()) grid_->set_tweights(tlink_s_.data(), tlink_t_.data());
+    // to the new graph as well
+    if (!tlink_s_.empty()) apply_tlinks();
   }
 
   void set_tweights(const EdgeWeight* capSource, const EdgeWeight* capSink) {
     tlink_s_ = detail::to_i32(capSource, (size_t)n_, "set_tweights");
     tlink_t_ = detail::to_i32(capSink, (size_t)n_, "set_tweights");
-    if (grid_) grid_->set_tweights(tlink_s_.data(), tlink_t_.data());
+    if (grid_ || generic_) apply_tlinks();
   }
 
   TFlow max_flow() {
@@ -183,12 +225,12 @@ class Graph {
   }
   template <typename TPolicy, typename TTraceObject>
   TFlow max_flow_with_tracing(TPolicy& policy, TTraceObject& trace) {
-    if (!grid_) throw Exception(CGC_ERR_STATE, "max_flow: set_nweights was not called");
+    if (!grid_ && !generic_) throw Exception(CGC_ERR_STATE, "max_flow: set_nweights was not called");
     cgc_stats before{};
     trace.computationStarted(before);
     const GraphCutPolicy& p = policy;
-    const int64_t f = grid_->max_flow(&p);
-    const cgc_stats st = grid_->stats();
+    const int64_t f = grid_ ? grid_->max_flow(&p) : generic_->max_flow(&p);
+    const cgc_stats st = grid_ ? grid_->stats() : generic_->stats();
     const std::vector<int> no_levels;
     for (int64_t i = 0; i < st.global_relabels; ++i) {
       trace.beginIteration((int)i);
@@ -213,27 +255,36 @@ class Graph {
   }
 
   GridGraph* grid() const { return grid_.get(); }
+  GenericGraph* generic() const { return generic_.get(); }
 
  private:
+  void apply_tlinks() {
+    if (grid_) grid_->set_tweights(tlink_s_.data(), tlink_t_.data());
+    else generic_->set_tweights(tlink_s_.data(), tlink_t_.data());
+  }
+
   template <typename THostArrayView>
   void fill(int which, THostArrayView& out, uint8_t mask, uint8_t background) const {
-    if (!grid_) throw Exception(CGC_ERR_STATE, "fill_segments: no graph");
-    std::vector<uint8_t> tmp(grid_->size());
-    grid_->segments(which, tmp.data(), mask, background);
+    if (!grid_ && !generic_) throw Exception(CGC_ERR_STATE, "fill_segments: no graph");
+    std::vector<uint8_t> tmp(grid_ ? grid_->size() : generic_->size());
+    if (grid_) grid_->segments(which, tmp.data(), mask, background);
+    else generic_->segments(which, tmp.data(), mask, background);
     for (size_t i = 0; i < tmp.size(); ++i) out[i] = tmp[i];
   }
 
-  struct GridPtr {
-    GridGraph* p = nullptr;
-    ~GridPtr() { delete p; }
-    void reset(GridGraph* q = nullptr) { delete p; p = q; }
-    GridGraph* get() const { return p; }
-    GridGraph* operator->() const { return p; }
+  template <typename T>
+  struct Owned {
+    T* p = nullptr;
+    ~Owned() { delete p; }
+    void reset(T* q = nullptr) { delete p; p = q; }
+    T* get() const { return p; }
+    T* operator->() const { return p; }
     explicit operator bool() const { return p != nullptr; }
   };
 
   int n_ = 0;
-  GridPtr grid_;
+  Owned<GridGraph> grid_;
+  Owned<GenericGraph> generic_;
   std::vector<int32_t> tlink_s_, tlink_t_;  // host copy of the last t-links
 };
 

@@ -1,6 +1,9 @@
 // Reference-style C++ use of the cgc facade: the 4x4 graph of the reference's
 // test/graph_cut.cu:13-67 through cgc::Graph<float> (the reference's float
-// API), the same through Graph<int>, and a grid through cgc::GridGraph.
+// API), the same through Graph<int>, the layered graphs of the reference's
+// unit_tests/graph_cut_test.cu:22-65,172-198 (known flows 1024*8 and
+// 2*1024*8; not a grid, so the generic engine solves them) and a grid through
+// cgc::GridGraph.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -48,9 +51,48 @@ void four_by_four() {
   EXPECT(graph.max_flow() == (W)4);
 }
 
+// layers of `size` vertices; vertex i of a layer joins vertices i..i+nbrs-1
+// (mod size) of the next layer with weight 20 forward, 40 backward, except a
+// 1 / 2 bottleneck at the middle layer; terminals on the first and last layer
+template <typename W>
+void layered(bool flip, long long expected) {
+  const int layers = 100, size = 1024, nbrs = 8;
+  cgc::Graph<W> graph;
+  graph.set_vertex_count(layers * size);
+  std::vector<cgc::EdgeRecord> edges;
+  std::vector<W> fw, bw;
+  for (int layer = 1; layer < layers; ++layer) {
+    const W weight = layer == layers / 2 ? (W)1 : (W)20;
+    for (int i = 0; i < size; ++i)
+      for (int j = 0; j < nbrs; ++j) {
+        edges.emplace_back((layer - 1) * size + i, layer * size + (i + j) % size);
+        fw.push_back(weight);
+        bw.push_back(2 * weight);
+      }
+  }
+  std::vector<W> first(layers * size, (W)0), last(layers * size, (W)0);
+  for (int i = 0; i < size; ++i) {
+    first[i] = (W)100000;
+    last[(layers - 1) * size + i] = (W)100000;
+  }
+  graph.set_nweights((int)edges.size(), edges.data(), fw.data(), bw.data());
+  if (flip) graph.set_tweights(last.data(), first.data());
+  else graph.set_tweights(first.data(), last.data());
+  EXPECT(graph.generic() != nullptr && graph.grid() == nullptr);
+  EXPECT((long long)graph.max_flow() == expected);
+  std::vector<unsigned char> seg(layers * size);
+  graph.fill_segments(seg.data());
+  // the bottleneck layer separates the sides
+  const int sink_first = flip ? 0 : (layers / 2) * size;
+  EXPECT(seg[sink_first] == 255 && seg[flip ? (layers - 1) * size : 0] == 0);
+}
+
 int main() {
   four_by_four<float>();
   four_by_four<int>();
+  layered<float>(false, 1024 * 8);
+  layered<float>(true, 2 * 1024 * 8);
+  layered<int>(false, 1024 * 8);
   // non-integral weights are rejected
   bool threw = false;
   try {

@@ -54,13 +54,17 @@ def test_reference_four_by_four_through_graph_api():
     assert G.fill_segments(mask=1, which=SOURCE).tolist() == [1] * 8 + [0] * 8
 
 
-def test_layered_reference_graph_is_rejected_loudly():
+def test_layered_reference_graph_goes_to_the_generic_engine():
     n, a, b, f, g, s, t = graphs.layered(layers=6, size=32, nbrs=4)
     G = Graph()
     G.set_vertex_count(n)
-    with pytest.raises(_lib.CgcError) as e:
-        G.set_nweights(len(a), np.stack([a, b], 1), f, g)
-    assert e.value.code == 8
+    G.set_nweights(len(a), np.stack([a, b], 1), f, g)
+    G.set_tweights(s, t)
+    assert G.generic is not None and G.grid is None
+    f0, s0, t0, _ = oracle.maxflow_edges(n, a, b, f, g, s, t)
+    assert G.max_flow() == f0
+    assert np.array_equal(G.fill_segments(mask=1, which=SOURCE), s0)
+    assert np.array_equal(G.fill_segments(mask=1, which=SINK), t0)
 
 
 @pytest.mark.parametrize("policy", list(POLICIES))
