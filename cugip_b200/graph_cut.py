@@ -6,8 +6,9 @@ set_vertex_count / set_nweights(edge list) / set_tweights / max_flow /
 fill_segments, with int32 capacities and an exact int flow.  `GridGraph` is
 the grid-native form: t-link volumes and one n-link volume per axis, which is
 what the reference's grid front-end builds
-(benchmarks/graph_cut/graph_cut.cpp:33-98).  `Batch` solves many grids of
-uneven sizes in one launch.
+(benchmarks/graph_cut/graph_cut.cpp:33-98).  `GenericGraph` takes any edge
+list (the generic engine `Graph` falls back to when the edges do not form a
+grid).  `Batch` solves many grids of uneven sizes in one launch.
 
 Every solve runs on the GPU through libcgc.so; nothing here computes a flow.
 """
