@@ -195,6 +195,18 @@ __global__ void k_csr_prepare(CsrDev D) {
     D.h[v] = 0;
     D.stamp[v] = 0;
     through += mn;
+    // Excess and residuals stay int32: the excess is at most the source
+    // excess plus every capacity into v, a residual at most the two
+    // capacities of its edge.
+    long long inflow = s - mn;
+    bool bad = false;
+    const int a1 = D.row[v + 1];
+    for (int a = D.row[v]; a < a1; ++a) {
+      const long long back = D.res0[D.rev[a]];
+      inflow += back;
+      if (back + D.res0[a] > 2147483647ll) bad = true;
+    }
+    if (bad || inflow > 2147483647ll) atomicCAS(D.err, 0, CGC_ERR_OVERFLOW);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) through += __shfl_down_sync(0xffffffffu, through, o);
@@ -569,6 +581,8 @@ int graph_maxflow(cgc_graph* g, const cgc_options* opts, int64_t* flow) {
     CGC_CUDA(cudaMemcpy(&err, d.err, 4, cudaMemcpyDeviceToHost));
     if (err == CGC_ERR_TIMEOUT) return fail(CGC_ERR_TIMEOUT, "cgc_graph_maxflow: a grid barrier timed out");
     if (err == CGC_ERR_NOT_CONVERGED) return fail(CGC_ERR_NOT_CONVERGED, "cgc_graph_maxflow: pulse cap reached");
+    if (err == CGC_ERR_OVERFLOW)
+      return fail(CGC_ERR_OVERFLOW, "cgc_graph_maxflow: capacities may overflow int32 excess or residuals");
     if (err) return fail(err, "cgc_graph_maxflow: device error");
     unsigned long long f = 0, stats[CS_N];
     CGC_CUDA(cudaMemcpy(&f, d.flow, 8, cudaMemcpyDeviceToHost));

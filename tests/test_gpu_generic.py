@@ -132,6 +132,24 @@ def test_terminal_only_vertices_and_isolated_vertices():
     assert np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
+def test_capacities_that_could_overflow_int32_are_refused():
+    big = 2 ** 30 + 1
+    with GenericGraph(3, [0, 1], [1, 2], [big, 1], [big, 1]) as G:  # one edge's two capacities exceed int32
+        G.set_tweights([5, 0, 0], [0, 0, 5])
+        with pytest.raises(_lib.CgcError) as e:
+            G.max_flow()
+        assert e.value.code == 6
+    hub = np.zeros(3, np.int64)  # vertex 0 can receive 3 * 2^30: more than int32 excess
+    with GenericGraph(4, hub, [1, 2, 3], [0, 0, 0], [2 ** 30] * 3) as G:
+        G.set_tweights([0, 9, 9, 9], [9, 0, 0, 0])
+        with pytest.raises(_lib.CgcError) as e:
+            G.max_flow()
+        assert e.value.code == 6
+    with GenericGraph(2, [0], [1], [2 ** 30], [2 ** 30 - 1]) as G:  # at the limit: fine
+        G.set_tweights([2 ** 30, 0], [0, 2 ** 30])
+        assert G.max_flow() == 2 ** 30
+
+
 def test_errors_are_loud():
     with pytest.raises(_lib.CgcError) as e:
         GenericGraph(4, [0, 5], [1, 2], [1, 1], [1, 1])
