@@ -165,8 +165,8 @@ __global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
 }
 
 __global__ void __launch_bounds__(512) k_bfs_init(DevPool P) {
-  __shared__ BfsShared S;
-  for (int t = blockIdx.x; t < P.T; t += gridDim.x) bfs_init_tile(P, t, S);
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < P.T; t += nw) bfs_init_tile_w(P, t);
 }
 
 __global__ void k_bfs_queue(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(512, 2) k_bfs_round(DevPool P, const int32_t* 
 }
 
 __global__ void __launch_bounds__(512) k_reach_init(DevPool P, uint32_t id0, int32_t* list0, int32_t* cnt0) {
-  __shared__ ReachShared S;
-  for (int t = blockIdx.x; t < P.T; t += gridDim.x) reach_init_tile(P, t, S, id0, list0, cnt0);
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < P.T; t += nw)
+    reach_init_tile_w(P, t, id0, list0, cnt0);
 }
 
 __global__ void __launch_bounds__(512, 2) k_reach_round(DevPool P, const int32_t* list, const int32_t* cnt, uint32_t id_next,
@@ -272,6 +273,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   const int U = WARP ? G * (int)(blockDim.x >> 5) : G;
   const int u = WARP ? b * (int)(blockDim.x >> 5) + (tid >> 5) : b;
   const bool leader = WARP ? (tid & 31) == 0 : tid == 0;
+  // warps of the grid, for the passes that visit every tile with a warp
+  const int gw = b * (int)(blockDim.x >> 5) + (tid >> 5), nw = G * (int)(blockDim.x >> 5);
   int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
   int32_t* const sl[4] = {P.lists + 3 * P.T, P.lists + 4 * P.T, P.lists + 5 * P.T, P.lists + 6 * P.T};
   int32_t* const bc = P.cnt + C_BFS0;
@@ -306,10 +309,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
     }
     if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = u; t < P.T; t += U) {
-      if constexpr (WARP) bfs_init_tile_w(P, t);
-      else bfs_init_tile(P, t, S.bfs);
-    }
+    for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);  // a warp per tile in both shapes
     if (!grid_sync(P, prm.limit_ns)) return;
     for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x) bfs_queue_tile(P, t0 + tid, bfs_id, bl[0], bc + 0);
     if (!grid_sync(P, prm.limit_ns)) return;
@@ -407,10 +407,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   // ------------------------------------------------ source-side reachability
   if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
   if (!grid_sync(P, prm.limit_ns)) return;
-  for (int t = u; t < P.T; t += U) {
-    if constexpr (WARP) reach_init_tile_w(P, t, bfs_id, bl[0], bc + 0);
-    else reach_init_tile(P, t, S.rc, bfs_id, bl[0], bc + 0);
-  }
+  for (int t = gw; t < P.T; t += nw) reach_init_tile_w(P, t, bfs_id, bl[0], bc + 0);
   if (!grid_sync(P, prm.limit_ns)) return;
   int k = 0;
   for (;;) {
@@ -454,6 +451,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
 __device__ __forceinline__ void solve_async(const DevPool& P, const SolveParams& prm, SolveShared& S) {
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   const int gtid = b * blockDim.x + tid, nthr = G * blockDim.x;
+  const int gw = b * (int)(blockDim.x >> 5) + (tid >> 5), nw = G * (int)(blockDim.x >> 5);
   __shared__ int s_take;
   // queue A: BFS and reachability; queue B: push-relabel visits
   const WorkQueue qa{P.qring, P.qcap, P.qctl, prm.limit_ns};
@@ -536,7 +534,7 @@ __device__ __forceinline__ void solve_async(const DevPool& P, const SolveParams&
     // ------------------------------------------------ exact global relabel
     reset_queues();
     if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = b; t < P.T; t += G) bfs_init_tile(P, t, S.bfs);
+    for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);
     if (!grid_sync(P, prm.limit_ns)) return;
     ++bfs_id;
     for (int t = gtid; t < P.T; t += nthr)
@@ -586,7 +584,7 @@ __device__ __forceinline__ void solve_async(const DevPool& P, const SolveParams&
   reset_queues();
   if (!grid_sync(P, prm.limit_ns)) return;
   ++bfs_id;
-  for (int t = b; t < P.T; t += G) reach_init_tile(P, t, S.rc, bfs_id, nullptr, nullptr, &qa);
+  for (int t = gw; t < P.T; t += nw) reach_init_tile_w(P, t, bfs_id, nullptr, nullptr, &qa);
   if (!grid_sync(P, prm.limit_ns)) return;
   drain(qa, 2, bfs_id, 0);
   if (!grid_sync(P, prm.limit_ns)) return;

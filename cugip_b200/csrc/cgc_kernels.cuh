@@ -332,38 +332,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 }
 
 // ---------------------------------------------------------------------------
-// BFS seed for tile t: h = 1 where the sink residual is positive, INF elsewhere.
-// A tile with seeds is queued, and so is every face neighbour next to a seed
-// on the tile's face (the neighbour reads the seed through its halo).
-__device__ inline void bfs_init_tile(const DevPool& P, const int t, BfsShared& S) {
-  const int l = threadIdx.x;
-  const int64_t g = (int64_t)t * TV + l;
-  const unsigned rm = __ldcg(P.rmask + g);
-  const bool seed = (rm & 64u) != 0;
-  // A tile whose voxels were all found unable to reach the sink stays so
-  // (dead vertices neither receive nor send flow, and all their residual
-  // neighbours are dead), so it keeps INF and is never visited again.
-  // Heights are 0 before the first relabel of a solve.
-  const int dead = __syncthreads_and(__ldcg(P.h + g) == INF);
-  if (dead) {
-    if (l == 0) { P.tflag[t] = TF_DEAD; P.act[t] = 0; }
-    return;
-  }
-  P.h[g] = seed ? 1 : INF;
-  if (l == 0) S.flags = 0;
-  __syncthreads();
-  if (seed) atomicOr(&S.flags, (face_bits(l & 7, (l >> 3) & 7, l >> 6) << 1) | TF_HAS_SEED);
-  const int all_seed = __syncthreads_and(seed);
-  // a tile whose voxels are all seeds is final at h = 1 and is never visited
-  int act = 0;
-  if (all_seed) act = __syncthreads_or((rm & 128u) != 0);
-  if (l == 0) {
-    P.tflag[t] = (uint16_t)(S.flags | (all_seed ? TF_ALL_SEED : 0));
-    P.act[t] = (uint8_t)(act ? 1 : 0);
-  }
-  __syncthreads();
-}
-
+// BFS seeding, first step: bfs_init_tile_w (a warp per tile).
 // Second BFS seeding step, one thread per tile: queue every tile that is not
 // all seeds and holds a seed or touches a seed on a neighbour's face.
 __device__ __forceinline__ bool bfs_seed_tile(const DevPool& P, const int t) {
@@ -443,29 +412,8 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
 
 // ---------------------------------------------------------------------------
 // Source-side reachability (canonical cut) after the maximum preflow:
-// closure of {v : e(v) > 0} over residual edges.
-__device__ inline void reach_init_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id0, int32_t* list0,
-                                int32_t* cnt0, const WorkQueue* wq = nullptr) {
-  const int l = threadIdx.x;
-  const int64_t g = (int64_t)t * TV + l;
-  const bool seed = (__ldcg(P.rmask + g) & 128u) != 0;
-  P.reach[g] = seed ? 1 : 0;
-  if (l == 0) S.flags = 0;
-  __syncthreads();
-  if (seed) {
-    const int fb = face_bits(l & 7, (l >> 3) & 7, l >> 6);
-    atomicOr(&S.flags, fb | 64);
-  }
-  __syncthreads();
-  const int fl = S.flags;
-  if (l == 0 && (fl & 64)) enqueue(P, P.stamp_bfs, t, id0, list0, cnt0, wq);
-  if (l < 6 && ((fl >> l) & 1)) {
-    const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id0, list0, cnt0, wq);
-  }
-  __syncthreads();
-}
-
+// closure of {v : e(v) > 0} over residual edges, seeded by reach_init_tile_w
+// (a warp per tile).
 __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
                            int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
   const int l = threadIdx.x;

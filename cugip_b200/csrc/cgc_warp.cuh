@@ -1,4 +1,7 @@
-// Warp-per-tile variants of the tile routines.
+// Warp-per-tile variants of the tile routines.  The seeding passes over all
+// tiles (bfs_init_tile_w, reach_init_tile_w) are also what the 512-thread
+// kernels use: a warp per tile needs no block barrier, so a CTA seeds 16
+// tiles at a time.
 //
 // One warp owns one 8x8x8 tile: lane l owns the 16 voxels l + 32k
 // (k = 0..15), i.e. x = l&7, y = ((l>>3)&3) + 4(k&1), z = k>>1.  The tile's
@@ -280,6 +283,14 @@ __device__ inline void sweep_tile_w(const DevPool& P, const int t, const int L, 
 }
 
 // ---------------------------------------------------------------------------
+// BFS seed for tile t: h = 1 where the sink residual is positive, INF
+// elsewhere; the tile's seed summary (face bits, any seed, all seeds) goes to
+// tflag for the second seeding step (bfs_seed_tile / bfs_queue_tile).
+// A tile whose voxels were all found unable to reach the sink stays so (dead
+// vertices neither receive nor send flow, and all their residual neighbours
+// are dead), so it keeps INF and is never visited again; heights are 0 before
+// the first relabel of a solve.  A tile whose voxels are all seeds is final
+// at h = 1 and is never visited.
 __device__ inline void bfs_init_tile_w(const DevPool& P, const int t) {
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
@@ -376,8 +387,10 @@ __device__ inline void bfs_tile_w(const DevPool& P, const int t, WarpBfsSmem& S,
 }
 
 // ---------------------------------------------------------------------------
+// Reachability seed for tile t: the voxels holding excess; the tile is queued
+// if it has one, and so is every face neighbour next to one.
 __device__ inline void reach_init_tile_w(const DevPool& P, const int t, const uint32_t id0, int32_t* list0,
-                                         int32_t* cnt0) {
+                                         int32_t* cnt0, const WorkQueue* wq = nullptr) {
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
   unsigned flags = 0;
@@ -389,10 +402,10 @@ __device__ inline void reach_init_tile_w(const DevPool& P, const int t, const ui
     if (seed) flags |= face_bits(wv_x(lane), wv_y(lane, k), wv_z(k)) | 64u;
   }
   flags = __reduce_or_sync(FULL, flags);
-  if (lane == 0 && (flags & 64u)) queue_tile(P, P.stamp_bfs, t, id0, list0, cnt0);
+  if (lane == 0 && (flags & 64u)) enqueue(P, P.stamp_bfs, t, id0, list0, cnt0, wq);
   if (lane < 6 && ((flags >> lane) & 1)) {
     const int nt = __ldcg(P.nbr + lane * P.T + t);
-    if (nt >= 0) queue_tile(P, P.stamp_bfs, nt, id0, list0, cnt0);
+    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id0, list0, cnt0, wq);
   }
 }
 
