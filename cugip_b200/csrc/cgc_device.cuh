@@ -38,6 +38,7 @@ enum Counter {
   C_ACT = 7,       // active tiles after the last global relabel
   C_ROUNDS = 8,    // BFS rounds executed
   C_SINKT0 = 9,    // 3 slots: tiles that delivered flow to the sink in a sweep
+  C_TAKE0 = 12,    // 3 slots: next list entry to hand out in a round (persistent solve)
   C_NCOUNTERS = 16
 };
 

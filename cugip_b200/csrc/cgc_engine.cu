@@ -275,6 +275,32 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   const bool leader = WARP ? (tid & 31) == 0 : tid == 0;
   // warps of the grid, for the passes that visit every tile with a warp
   const int gw = b * (int)(blockDim.x >> 5) + (tid >> 5), nw = G * (int)(blockDim.x >> 5);
+  // Hands out the n entries of a round.  CTA shape: the first entry of CTA b
+  // is entry b; later ones come from the round's counter (C_TAKE0 + round % 3,
+  // the next round's slot is cleared meanwhile) through an atomic issued when
+  // the current visit starts and read when it ends, so visits of uneven cost
+  // spread over the CTAs.  Warp shape: static striding.
+  __shared__ int s_next;
+  int round_no = 0;
+  auto for_entries = [&](int n, auto&& visit) {
+    if constexpr (WARP) {
+      for (int i = u; i < n; i += U) visit(i);
+    } else {
+      int32_t* take = P.cnt + C_TAKE0 + round_no % 3;
+      if (b == 0 && tid == 0) P.cnt[C_TAKE0 + (round_no + 1) % 3] = 0;
+      ++round_no;
+      int i = b;
+      while (i < n) {
+        int nx = 0;
+        if (tid == 0) nx = atomicAdd(take, 1);
+        visit(i);
+        if (tid == 0) s_next = G + nx;
+        __syncthreads();
+        i = s_next;
+        __syncthreads();
+      }
+    }
+  };
   int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
   int32_t* const sl[4] = {P.lists + 3 * P.T, P.lists + 4 * P.T, P.lists + 5 * P.T, P.lists + 6 * P.T};
   int32_t* const bc = P.cnt + C_BFS0;
@@ -307,7 +333,9 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       bc[0] = bc[1] = bc[2] = 0;
       sc[0] = sc[1] = sc[2] = sc[3] = 0;
       P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
+      P.cnt[C_TAKE0] = P.cnt[C_TAKE0 + 1] = P.cnt[C_TAKE0 + 2] = 0;
     }
+    round_no = 0;
     if (!grid_sync(P, prm.limit_ns)) return;
     for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);  // a warp per tile in both shapes
     if (!grid_sync(P, prm.limit_ns)) return;
@@ -318,10 +346,10 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const int n = ld_cnt(bc + k % 3);
       if (n == 0) break;
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-      for (int i = u; i < n; i += U) {
+      for_entries(n, [&](int i) {
         if constexpr (WARP) bfs_tile_w(P, __ldcg(bl[k % 3] + i), W.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
         else bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-      }
+      });
       ++k;
       if (!grid_sync(P, prm.limit_ns)) return;
       record(TR_BFS_ROUND, rounds + k, n);
@@ -376,12 +404,12 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       // the learned scheduler defers low-priority tiles during the first half
       // of the cycle; every active tile is swept in the second half
       const bool may_defer = learned && prm.learned == 1 && j < prm.K;
-      for (int i = u; i < n; i += U) {
+      for_entries(n, [&](int i) {
         const int t = __ldcg(sl[s & 3] + i);
         if (may_defer && !__ldcg(P.sprio + t)) {
           if (leader && atomicExch(P.stamp_sw + t, (uint32_t)(s + 3)) != (uint32_t)(s + 3))
             sl[(s + 2) & 3][atomicAdd(sc + ((s + 2) & 3), 1)] = t;
-          continue;
+          return;
         }
         const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
         if constexpr (WARP)
@@ -390,7 +418,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
         else
           sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
                            (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
-      }
+      });
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
       record(TR_SWEEP, sweeps, n);
@@ -405,7 +433,11 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   }
   lap(ns_bfs);
   // ------------------------------------------------ source-side reachability
-  if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
+  if (b == 0 && tid == 0) {
+    bc[0] = bc[1] = bc[2] = 0;
+    P.cnt[C_TAKE0] = P.cnt[C_TAKE0 + 1] = P.cnt[C_TAKE0 + 2] = 0;
+  }
+  round_no = 0;
   if (!grid_sync(P, prm.limit_ns)) return;
   for (int t = gw; t < P.T; t += nw) reach_init_tile_w(P, t, bfs_id, bl[0], bc + 0);
   if (!grid_sync(P, prm.limit_ns)) return;
@@ -414,10 +446,10 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     const int n = ld_cnt(bc + k % 3);
     if (n == 0) break;
     if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-    for (int i = u; i < n; i += U) {
+    for_entries(n, [&](int i) {
       if constexpr (WARP) reach_tile_w(P, __ldcg(bl[k % 3] + i), W.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
       else reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-    }
+    });
     ++k;
     if (!grid_sync(P, prm.limit_ns)) return;
     record(TR_REACH_ROUND, k, n);
