@@ -360,12 +360,13 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     lap(ns_bfs);
     // ------------------------------------------------ active tiles -> parity lists
     s += 2;  // fresh stamp ids for the lists built here
-    for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
-      if (__ldcg(P.act + t)) {
-        const int par = __ldcg(P.tpar + t);
-        P.stamp_sw[t] = (uint32_t)(s + par + 1);
-        sl[(s + par) & 3][atomicAdd(sc + ((s + par) & 3), 1)] = t;
-      }
+    for (int t0 = b * blockDim.x + (tid & ~31); t0 < P.T; t0 += G * blockDim.x) {  // warp-aggregated appends
+      const int t = t0 + (tid & 31);
+      const bool a = t < P.T && __ldcg(P.act + t);
+      const int par = a ? __ldcg(P.tpar + t) : 0;
+      if (a) P.stamp_sw[t] = (uint32_t)(s + par + 1);
+      warp_append(a && par == 0, t, sl[s & 3], sc + (s & 3));
+      warp_append(a && par == 1, t, sl[(s + 1) & 3], sc + ((s + 1) & 3));
     }
     if (!grid_sync(P, prm.limit_ns)) return;
     const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));

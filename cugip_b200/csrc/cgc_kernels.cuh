@@ -144,21 +144,20 @@ __device__ __forceinline__ long long block_sum64(long long v, long long* red) {
 struct SweepShared {
   int h[2][HALO];
   int out[2][6][TV];
-  long long red[16];
+  unsigned long long sink;  // flow delivered to the sink by this visit
+  int nb[6];                // face neighbours of the tile (-1 outside)
   int flags;
   int lastout;  // last pulse (1-based) that moved flow out of the tile or into the sink
 };
 
 struct BfsShared {
   int h[2][HALO];
-  long long red[16];
   int flags;
 };
 
 struct ReachShared {
   unsigned char rc[2][HALO];
   unsigned char m[HALO];
-  long long red[16];
   int flags;
 };
 
@@ -192,7 +191,8 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
   load_halo_heights(P, t, S.h);
   const int inst = __ldcg(P.tinst + t);
   const int hdead = P.geo[inst].hdead;
-  if (l == 0) { S.flags = 0; S.lastout = 0; }
+  if (l < 6) S.nb[l] = __ldcg(P.nbr + l * P.T + t);  // read by the write-back
+  if (l == 0) { S.flags = 0; S.lastout = 0; S.sink = 0ull; }
   __syncthreads();
 
   int acc[6] = {0, 0, 0, 0, 0, 0};  // flow pushed out of the tile, per face
@@ -294,7 +294,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 #pragma unroll
   for (int d = 0; d < 6; ++d) {
     if (!inside(d, x, y, z) && acc[d] > 0) {
-      const int nt = __ldcg(P.nbr + d * P.T + t);
+      const int nt = S.nb[d];
       if (nt < 0) { raise_error(P, CGC_ERR_OVERFLOW); continue; }  // capacity leaving the grid
       const int64_t ng = (int64_t)nt * TV + l + xoff(d);
       atomicAdd(P.e + ng, acc[d]);
@@ -303,12 +303,17 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
       atomicOr(&S.flags, 1 << d);
     }
   }
+  // sink flow of the visit: warp sums into one shared total before the barrier
+  unsigned long long ws = (unsigned long long)sink;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ws += __shfl_down_sync(0xffffffffu, ws, o);
+  if ((l & 31) == 0 && ws) atomicAdd(&S.sink, ws);
   const int still = __syncthreads_or(e > 0 && h < INF);
-  const long long total = block_sum64((long long)sink, S.red);
+  const unsigned long long total = S.sink;
   if (l == 0) {
     P.act[t] = (uint8_t)(still ? 1 : 0);
     if (total) {
-      atomicAdd(P.flow + inst, (unsigned long long)total);
+      atomicAdd(P.flow + inst, total);
       if (ex.sink_tiles) atomicAdd(ex.sink_tiles, 1);
       if (ex.tr_sink) ex.tr_sink[t] = 1;
     }
@@ -322,9 +327,11 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
     if (wq) tile_unlock(P, t);
   }
   if (wq) __syncthreads();
-  if (APPEND && l == 0 && still) enqueue(P, P.stamp_sw, t, id_self, list_self, cnt_self, wq);
+  // the tile re-queues itself from another warp than thread 0's face chain,
+  // so the two dependent atomic chains overlap
+  if (APPEND && l == 32 && still) enqueue(P, P.stamp_sw, t, id_self, list_self, cnt_self, wq);
   if (l < 6 && ((S.flags >> l) & 1)) {
-    const int nt = __ldcg(P.nbr + l * P.T + t);
+    const int nt = S.nb[l];
     P.act[nt] = 1;
     if (APPEND) enqueue(P, P.stamp_sw, nt, id_next, list_next, cnt_next, wq);
   }
@@ -369,6 +376,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
                          int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
+  const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
   int h = __ldcg(P.h + g);
@@ -403,10 +411,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
     if (act) P.act[t] = 1;
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
   }
-  if (l < 6 && ((S.flags >> l) & 1)) {
-    const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id_next, list_next, cnt_next, wq);
-  }
+  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) enqueue(P, P.stamp_bfs, nb, id_next, list_next, cnt_next, wq);
   __syncthreads();
 }
 
@@ -417,6 +422,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
 __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
                            int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
   const int l = threadIdx.x;
+  const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
   int rc = __ldcg(P.reach + g);
@@ -457,10 +463,7 @@ __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S,
     if (fb) atomicOr(&S.flags, fb);
   }
   __syncthreads();
-  if (l < 6 && ((S.flags >> l) & 1)) {
-    const int nt = __ldcg(P.nbr + l * P.T + t);
-    if (nt >= 0) enqueue(P, P.stamp_bfs, nt, id_next, list_next, cnt_next, wq);
-  }
+  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) enqueue(P, P.stamp_bfs, nb, id_next, list_next, cnt_next, wq);
   __syncthreads();
 }
 
