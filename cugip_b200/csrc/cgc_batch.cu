@@ -21,8 +21,13 @@
 namespace cgc {
 
 // Upload of every instance from its bound device inputs (8 pointers per
-// instance: capS, capT, fwd x/y/z, bwd x/y/z; a null n-link pointer is zero).
+// instance: capS, capT, fwd x/y/z, bwd x/y/z; a null n-link pointer is zero),
+// fused with the preflow initialisation of k_prepare: every value that needs
+// (the capacity into the voxel from each neighbour: bwd[v] from +a,
+// fwd[v - stride] from -a) is an input this thread reads anyway, so the solve
+// starts after one pass over the planes instead of two.
 __global__ void __launch_bounds__(512) k_put_all(DevPool P, const int32_t* const* __restrict__ in) {
+  __shared__ long long red[16];
   const int t = blockIdx.x;
   const int inst = P.tinst[t];
   const InstGeo G = P.geo[inst];
@@ -32,7 +37,7 @@ __global__ void __launch_bounds__(512) k_put_all(DevPool P, const int32_t* const
   const int x = tx * 8 + (l & 7), y = ty * 8 + ((l >> 3) & 7), z = tz * 8 + (l >> 6);
   const int64_t g = (int64_t)t * TV + l;
   const int32_t* const* ip = in + 8 * inst;
-  int s = 0, c = 0, r[6] = {0, 0, 0, 0, 0, 0};
+  int s = 0, c = 0, r[6] = {0, 0, 0, 0, 0, 0}, back[6] = {0, 0, 0, 0, 0, 0};
   if (x < G.X && y < G.Y && z < G.Z) {
     const int64_t v = x + (int64_t)G.X * (y + (int64_t)G.Y * z);
     s = ip[0][v];
@@ -43,18 +48,45 @@ __global__ void __launch_bounds__(512) k_put_all(DevPool P, const int32_t* const
     for (int a = 0; a < 3; ++a) {
       const int32_t* f = ip[2 + a];
       const int32_t* b = ip[5 + a];
-      if (f && co[a] + 1 < ex[a]) r[2 * a] = f[v];
-      if (b && co[a] > 0) r[2 * a + 1] = b[v - st[a]];
+      if (co[a] + 1 < ex[a]) {
+        if (f) r[2 * a] = f[v];          // v -> v + e_a
+        if (b) back[2 * a] = b[v];       // v + e_a -> v
+      }
+      if (co[a] > 0) {
+        if (b) r[2 * a + 1] = b[v - st[a]];      // v -> v - e_a
+        if (f) back[2 * a + 1] = f[v - st[a]];   // v - e_a -> v
+      }
     }
     bool neg = s < 0 || c < 0;
 #pragma unroll
     for (int d = 0; d < 6; ++d) neg = neg || r[d] < 0;
     if (neg) raise_error(P, CGC_ERR_ARG);
   }
-  P.e[g] = s;
-  P.rT[g] = c;
+  // t-link cancellation: min(capS, capT) flows straight through
+  const int mcap = min(s, c);
+  const int e = s - mcap, rT = c - mcap;
+  long long inflow = e;
+  bool bad = false;
+  unsigned m = (rT > 0 ? 64u : 0u) | (e > 0 ? 128u : 0u);
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    inflow += back[d];
+    if ((long long)r[d] + back[d] > 2147483647ll) bad = true;
+    m |= (r[d] > 0 ? 1u : 0u) << d;
+  }
+  if (bad || inflow > 2147483647ll) raise_error(P, CGC_ERR_OVERFLOW);
+  P.e[g] = e;
+  P.rT[g] = rT;
 #pragma unroll
   for (int d = 0; d < 6; ++d) P.r[d * P.Np + g] = r[d];
+  P.h[g] = 0;  // no label yet (INF would read as "dead" to the first global relabel)
+  P.rmask[g] = (uint8_t)m;
+  P.reach[g] = 0;
+  const long long tot = block_sum64((long long)mcap, red);
+  if (l == 0) {
+    P.act[t] = 0;
+    if (tot) atomicAdd(P.flow + inst, (unsigned long long)tot);
+  }
 }
 
 // Both cut sets of every instance into its bound device outputs (1/0 bytes).
@@ -130,8 +162,6 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, stream));
   k_put_all<<<d.T, 512, 0, stream>>>(d, p.d_in);
-  note_launch();
-  k_prepare<<<d.T, 512, 0, stream>>>(d);
   note_launch();
   SolveParams prm;
   prm.L = o.local_pulses;

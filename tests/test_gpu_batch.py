@@ -117,3 +117,40 @@ def test_sharded_solve_single_rank_matches_golden():
     vols = [volume.workload(*k) for k in keys]
     flows = solve_sharded([(v.X, v.Y, v.Z) for v in vols], lambda idx: solve_batch_on_rank([vols[i] for i in idx]))
     assert flows == [CASES[k]["flow"] for k in keys]
+
+
+def test_bound_inputs_are_checked_like_host_uploads():
+    """The device-resident path refuses negative capacities and capacities
+    that could overflow int32 excess or residuals, like the host setters, and
+    matches the oracle on asymmetric bound n-links."""
+    import torch
+    from cugip_b200 import _lib
+    from oracle import oracle  # the checker
+    from tests import graphs
+    dev = torch.device("cuda", 0)
+    X, Y, Z = 11, 9, 5
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, 77)
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (capS, capT, *fwd, *bwd)]
+    out = (torch.zeros(X * Y * Z, dtype=torch.uint8, device=dev), torch.zeros(X * Y * Z, dtype=torch.uint8, device=dev))
+    B = Batch([(X, Y, Z)])
+    try:
+        B.bind_inputs(0, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:5]],
+                      [t.data_ptr() for t in d[5:8]])
+        B.bind_outputs(0, out[0].data_ptr(), out[1].data_ptr())
+        B.enqueue(Policy())
+        assert B.wait() == [f0]
+        assert np.array_equal(out[0].cpu().numpy(), s0) and np.array_equal(out[1].cpu().numpy(), t0)
+        d[2][7] = -3  # a negative n-link
+        B.enqueue(Policy())
+        with pytest.raises(_lib.CgcError) as e:
+            B.wait()
+        assert e.value.code == 1
+        d[2][7] = 2 ** 30  # both directions of one link: more than int32 together
+        d[5][7] = 2 ** 30
+        B.enqueue(Policy())
+        with pytest.raises(_lib.CgcError) as e:
+            B.wait()
+        assert e.value.code == 6
+    finally:
+        B.close()
