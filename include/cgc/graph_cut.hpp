@@ -122,6 +122,28 @@ class GridGraph {
     check(cgc_grid_stats(g_, &s), "stats");
     return s;
   }
+  // Phase records of the last persistent solve (cgc_grid_trace): kind 1 = BFS
+  // round, 2 = global relabel done (tiles = active tiles), 3 = sweep, 4 =
+  // reachability round; `tiles` = tiles in the round; `ns` since the launch.
+  struct PhaseRecord {
+    int kind;
+    int64_t index;
+    int tiles;
+    int64_t ns;
+  };
+  std::vector<PhaseRecord> trace() const {
+    int32_t n = 0;
+    check(cgc_grid_trace(g_, nullptr, 0, &n), "trace");
+    std::vector<int64_t> buf(2 * (size_t)n);
+    if (n > 0) check(cgc_grid_trace(g_, buf.data(), n, &n), "trace");
+    std::vector<PhaseRecord> out((size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+      const uint64_t w = (uint64_t)buf[2 * (size_t)i];
+      out[(size_t)i] = PhaseRecord{(int)(w >> 56), (int64_t)((w >> 24) & 0xffffffffu), (int)(w & 0xffffffu),
+                                   buf[2 * (size_t)i + 1]};
+    }
+    return out;
+  }
   cgc_grid* handle() const { return g_; }
 
  private:
@@ -231,11 +253,28 @@ class Graph {
     const GraphCutPolicy& p = policy;
     const int64_t f = grid_ ? grid_->max_flow(&p) : generic_->max_flow(&p);
     const cgc_stats st = grid_ ? grid_->stats() : generic_->stats();
-    const std::vector<int> no_levels;
-    for (int64_t i = 0; i < st.global_relabels; ++i) {
+    // One iteration per exact global relabel, as in the reference's MinCut
+    // loop (detail/graph_cut_implementation.hpp:150-175).  afterRelabel gets
+    // the level starts of that relabel's BFS: the running count of tiles
+    // visited per BFS round (the reference counts vertices per level); the
+    // push phase that follows is reported by afterPush.
+    std::vector<std::vector<int>> levels;
+    if (grid_) {
+      std::vector<int> cur{0};
+      for (const auto& r : grid_->trace()) {
+        if (r.kind == 1) {
+          cur.push_back(cur.back() + r.tiles);
+        } else if (r.kind == 2) {
+          levels.push_back(cur);
+          cur.assign(1, 0);
+        }
+      }
+    }
+    const int64_t iters = st.global_relabels;
+    for (int64_t i = 0; i < iters; ++i) {
       trace.beginIteration((int)i);
-      trace.afterRelabel((int)i, no_levels);
-      trace.afterPush((int)i, i + 1 == st.global_relabels, st);
+      trace.afterRelabel((int)i, i < (int64_t)levels.size() ? levels[(size_t)i] : std::vector<int>{0});
+      trace.afterPush((int)i, i + 1 == iters, st);
     }
     trace.computationFinished(static_cast<TFlow>(f), st);
     return static_cast<TFlow>(f);

@@ -16,9 +16,16 @@
   } while (0)
 
 struct CountingTrace : cgc::DummyTraceObject {
-  int iterations = 0;
+  int iterations = 0, relabels = 0, pushes = 0, last_levels = 0;
+  bool done_seen = false, levels_ok = true;
   long long finished = -1;
   void beginIteration(int) { ++iterations; }
+  void afterRelabel(int, const std::vector<int>& starts) {
+    ++relabels;
+    for (size_t i = 1; i < starts.size(); ++i) levels_ok = levels_ok && starts[i] >= starts[i - 1];
+    last_levels = (int)starts.size();
+  }
+  void afterPush(int, bool done, const cgc_stats&) { ++pushes; done_seen = done_seen || done; }
   template <typename T>
   void computationFinished(T flow, const cgc_stats&) { finished = (long long)flow; }
 };
@@ -40,6 +47,8 @@ void four_by_four() {
   W flow = graph.max_flow_with_tracing(trace);
   EXPECT(flow == (W)4);
   EXPECT(trace.finished == 4 && trace.iterations >= 1);
+  EXPECT(trace.relabels == trace.iterations && trace.pushes == trace.iterations && trace.done_seen);
+  EXPECT(trace.levels_ok && trace.last_levels >= 1);
   std::vector<unsigned char> seg(16);
   graph.fill_segments(seg.data());
   for (int i = 0; i < 16; ++i) EXPECT(seg[i] == (i < 8 ? 0 : 255));
