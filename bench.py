@@ -251,7 +251,7 @@ def main():
     B.bind_outputs(0, d_seg[0].data_ptr(), d_seg[1].data_ptr())
     cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr)
              for (L, R, K) in ((4, 2, 8), (2, 4, 4), (8, 2, 8), (4, 2, 16), (2, 4, 8), (4, 4, 8))
-             for c in (2, 3) for lr in ((0, 1) if have_learned else (0,))]
+             for c in (2, 3, 4) for lr in ((0, 1) if have_learned else (0,))]
     if args.schedule:
         L, R, K, c, lr = (int(x) for x in args.schedule.split(","))
         best, best_ms = Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr), None
@@ -434,7 +434,7 @@ def main():
             BB.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
             BB.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
         bcands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c)
-                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8)) for c in (2, 3)]
+                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8)) for c in (2, 3, 4)]
         bbest, _ = BB.autotune(bcands, repeats=1)
 
         def time_batch(pol, reps=3):

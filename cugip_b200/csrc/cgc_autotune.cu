@@ -5,8 +5,8 @@
 // graph_cut_policies.hpp:23-89).  Here the knobs are runtime options:
 // pulses per region-relabel round (L), region-relabel rounds per tile visit
 // (R), sweep pairs between exact global relabels (K) and the shape of the
-// persistent kernel (a 512-thread CTA per tile visit at 2 or 3 CTAs per SM, or
-// a warp per tile visit).  The autotuner times candidate
+// persistent kernel (a 512-thread CTA per tile visit at 2, 3 or 4 CTAs per SM,
+// or a warp per tile visit).  The autotuner times candidate
 // settings on the caller's own uploaded instance(s), keeps the fastest per size
 // class (instance count, voxel count) in a process-wide cache and, when the
 // environment variable CGC_AUTOTUNE_CACHE names a file, appends each result to
@@ -78,7 +78,7 @@ std::vector<cgc_options> default_candidates() {
   std::vector<cgc_options> c;
   // the warp-per-tile kernel is left out: it was 2-4x slower on every
   // measured workload (pass it as an explicit candidate to time it)
-  for (int cta : {2, 3})
+  for (int cta : {2, 3, 4})
     for (int R : {1, 2, 4})
       for (int L : {2, 4, 8})
         for (int K : {4, 8, 16}) {

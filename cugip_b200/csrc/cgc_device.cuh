@@ -134,6 +134,7 @@ __global__ void k_put_nlinks(DevPool P, int inst, int axis, const int32_t* __res
 __global__ void k_prepare(DevPool P);
 __global__ void k_solve(DevPool P, SolveParams prm);
 __global__ void k_solve3(DevPool P, SolveParams prm);
+__global__ void k_solve4(DevPool P, SolveParams prm);
 __global__ void k_solve_q(DevPool P, SolveParams prm);
 __global__ void k_solve_q3(DevPool P, SolveParams prm);
 constexpr int WARP_CTA_WARPS = 10;  // warps of the warp-per-tile solve CTA (one CTA per SM)

@@ -650,15 +650,16 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
     cfg.dynamicSmemBytes = kWarpSmemBytes;
     CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_w, d, prm));
   } else {
-    const bool three = o.ctas_per_sm == 3;
-    cfg.gridDim = dim3(three ? p.coop_blocks3 : p.coop_blocks);
+    const bool three = o.ctas_per_sm == 3, four = o.ctas_per_sm == 4 && !prm.async;
+    cfg.gridDim = dim3(four ? p.coop_blocks4 : three ? p.coop_blocks3 : p.coop_blocks);
     cfg.blockDim = dim3(512);
     cfg.dynamicSmemBytes = 0;
     if (prm.async) {
       if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q3, d, prm));
       else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q, d, prm));
     } else {
-      if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
+      if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve4, d, prm));
+      else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
       else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
     }
   }
@@ -671,6 +672,11 @@ __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   solve_body<false>(P, prm, &S);
 }
 __global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_body<false>(P, prm, &S);
+}
+// 4 CTAs per SM (2048 threads, 32 registers)
+__global__ void __launch_bounds__(512, 4) k_solve4(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
   solve_body<false>(P, prm, &S);
 }
@@ -839,6 +845,9 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   int occ3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_solve3, 512, 0));
   p->coop_blocks3 = std::max(1, occ3) * p->sms;
+  int occ4 = 0;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4, k_solve4, 512, 0));
+  p->coop_blocks4 = std::max(1, occ4) * p->sms;
   // the work-queue kernels have the same launch bounds; take the smaller grid
   int occq = 0, occq3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, k_solve_q, 512, 0));
@@ -915,7 +924,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->persistent) r.persistent = o->persistent;
     if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
-    if (o->ctas_per_sm == 2 || o->ctas_per_sm == 3) r.ctas_per_sm = o->ctas_per_sm;
+    if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
     r.warp_tiles = o->warp_tiles > 0 ? 1 : 0;
     r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;

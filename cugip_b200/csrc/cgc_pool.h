@@ -42,6 +42,7 @@ struct Pool {
   int sms = 148;
   int coop_blocks = 0;           // co-resident CTAs of k_solve
   int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
+  int coop_blocks4 = 0;          // co-resident CTAs of k_solve4
   int coop_blocks_w = 0;         // co-resident CTAs of k_solve_w
   int sweep_blocks = 0;
   cgc_stats st{};

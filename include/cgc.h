@@ -79,7 +79,7 @@ typedef struct cgc_options {
   int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
   int32_t region_relabels;    /* region-relabel rounds per tile visit (default 2, -1 = none) */
   int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
-  int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers) or 3 (40 registers) */
+  int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers), 3 (40) or 4 (32 registers) */
   int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
   int32_t warp_tiles;         /* persistent: 1 = one warp per tile visit (ten warps per SM), 0 = one 512-thread CTA */

@@ -29,6 +29,7 @@ POLICIES = {
     "host_R2": Policy(region_relabels=2, persistent=-1),
     "stall1_K64": Policy(stall_sweeps=1, sweeps_per_relabel=64),
     "stall3_L2": Policy(stall_sweeps=3, local_pulses=2, sweeps_per_relabel=16),
+    "cta4_R4": Policy(ctas_per_sm=4, region_relabels=4),
     "warp": Policy(warp_tiles=1),
     "warp_L1_K1": Policy(warp_tiles=1, local_pulses=1, sweeps_per_relabel=1),
     "warp_no_region": Policy(warp_tiles=1, region_relabels=-1, local_pulses=8),
@@ -95,7 +96,7 @@ def test_long_paths_match_oracle(seed):
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "warp", "async"])
+@pytest.mark.parametrize("policy", ["default", "cta4_R4", "warp", "async"])
 @pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 4, 5)])
 def test_golden_workloads(key, policy):
     c = CASES[key]
