@@ -53,6 +53,10 @@ __device__ __forceinline__ int xoff(int d) {
 __device__ __forceinline__ bool inside(int d, int x, int y, int z) {
   return d == PX ? x < 7 : d == MX ? x > 0 : d == PY ? y < 7 : d == MY ? y > 0 : d == PZ ? z < 7 : z > 0;
 }
+// entry of voxel (x,y,z) on face d in the order of for_halo_entry (a + 8b)
+__device__ __forceinline__ int face_entry(int d, int x, int y, int z) {
+  return (d == PX || d == MX) ? y + 8 * z : (d == PY || d == MY) ? x + 8 * z : x + 8 * y;
+}
 // bit mask of the faces of the tile the voxel lies on
 __device__ __forceinline__ int face_bits(int x, int y, int z) {
   return ((x == 7) << PX) | ((x == 0) << MX) | ((y == 7) << PY) | ((y == 0) << MY) | ((z == 7) << PZ) | ((z == 0) << MZ);
@@ -144,6 +148,7 @@ __device__ __forceinline__ long long block_sum64(long long v, long long* red) {
 struct SweepShared {
   int h[2][HALO];
   int out[2][6][TV];
+  int facc[6][64];          // flow pushed out of the tile per face entry (for_halo_entry order)
   unsigned long long sink;  // flow delivered to the sink by this visit
   int nb[6];                // face neighbours of the tile (-1 outside)
   int flags;
@@ -192,10 +197,10 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
   const int inst = __ldcg(P.tinst + t);
   const int hdead = P.geo[inst].hdead;
   if (l < 6) S.nb[l] = __ldcg(P.nbr + l * P.T + t);  // read by the write-back
+  if (l < 384) (&S.facc[0][0])[l] = 0;
   if (l == 0) { S.flags = 0; S.lastout = 0; S.sink = 0ull; }
   __syncthreads();
 
-  int acc[6] = {0, 0, 0, 0, 0, 0};  // flow pushed out of the tile, per face
   int sink = 0;
   int pulses = 0;
   int cur = 0;
@@ -231,26 +236,29 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
       int hn[6];
 #pragma unroll
       for (int d = 0; d < 6; ++d) hn[d] = S.h[cur][hi + hoff(d)];
-      int pushed[6] = {0, 0, 0, 0, 0, 0};
       bool moved_out = false;
-      if (e > 0 && h < INF) {
-        if (rT > 0 && h == 1) {
-          const int dl = min(e, rT);
-          e -= dl; rT -= dl; sink += dl;
-          moved_out = dl > 0;
-        }
-#pragma unroll
-        for (int d = 0; d < 6; ++d) {
-          if (e > 0 && r[d] > 0 && hn[d] == h - 1) {
-            const int dl = min(e, r[d]);
-            e -= dl; r[d] -= dl; pushed[d] = dl;
-          }
-        }
+      const bool act = e > 0 && h < INF;
+      if (act && rT > 0 && h == 1) {
+        const int dl = min(e, rT);
+        e -= dl; rT -= dl; sink += dl;
+        moved_out = dl > 0;
       }
+      // pushes; in-tile amounts (0 included) go to S.out for the receiver,
+      // amounts across a face to the face accumulator (this voxel is its
+      // only writer)
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
-        if (inside(d, x, y, z)) S.out[cur][d][l] = pushed[d];
-        else { acc[d] += pushed[d]; moved_out = moved_out || pushed[d] > 0; }
+        int dl = 0;
+        if (act && e > 0 && r[d] > 0 && hn[d] == h - 1) {
+          dl = min(e, r[d]);
+          e -= dl; r[d] -= dl;
+        }
+        if (inside(d, x, y, z)) {
+          S.out[cur][d][l] = dl;
+        } else if (dl > 0) {
+          S.facc[d][face_entry(d, x, y, z)] += dl;
+          moved_out = true;
+        }
       }
       if (moved_out) S.lastout = pulses + 1;  // same value from every writer of this pulse
       __syncthreads();
@@ -290,19 +298,20 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 #pragma unroll
   for (int d = 0; d < 6; ++d) { P.r[d * Np + g] = r[d]; m |= (r[d] > 0 ? 1u : 0u) << d; }
   P.rmask[g] = (uint8_t)m;
-  // flow that left the tile: excess and reverse residual of the neighbour
-#pragma unroll
-  for (int d = 0; d < 6; ++d) {
-    if (!inside(d, x, y, z) && acc[d] > 0) {
-      const int nt = S.nb[d];
-      if (nt < 0) { raise_error(P, CGC_ERR_OVERFLOW); continue; }  // capacity leaving the grid
-      const int64_t ng = (int64_t)nt * TV + l + xoff(d);
-      atomicAdd(P.e + ng, acc[d]);
-      atomicAdd(P.r + (d ^ 1) * Np + ng, acc[d]);
-      atomicOr((unsigned*)(P.rmask + (ng & ~(int64_t)3)), (128u | (1u << (d ^ 1))) << (8 * (int)(ng & 3)));
-      atomicOr(&S.flags, 1 << d);
+  // flow that left the tile: excess and reverse residual of the neighbour,
+  // one face entry per thread (the pulses ended with a barrier)
+  for_halo_entry(l, [&](int f, int, int src) {
+    const int a = (&S.facc[0][0])[l];
+    if (a > 0) {
+      const int nt = S.nb[f];
+      if (nt < 0) { raise_error(P, CGC_ERR_OVERFLOW); return; }  // capacity leaving the grid
+      const int64_t ng = (int64_t)nt * TV + src;
+      atomicAdd(P.e + ng, a);
+      atomicAdd(P.r + (f ^ 1) * Np + ng, a);
+      atomicOr((unsigned*)(P.rmask + (ng & ~(int64_t)3)), (128u | (1u << (f ^ 1))) << (8 * (int)(ng & 3)));
+      atomicOr(&S.flags, 1 << f);
     }
-  }
+  });
   // sink flow of the visit: warp sums into one shared total before the barrier
   unsigned long long ws = (unsigned long long)sink;
 #pragma unroll

@@ -55,10 +55,7 @@ __device__ __forceinline__ int wv_index(int lane, int k) { return lane + 32 * k;
 __device__ __forceinline__ int wv_x(int lane) { return lane & 7; }
 __device__ __forceinline__ int wv_y(int lane, int k) { return ((lane >> 3) & 3) | ((k & 1) << 2); }
 __device__ __forceinline__ int wv_z(int k) { return k >> 1; }
-// entry of voxel (x,y,z) on face d in the order of for_halo_entry (a + 8b)
-__device__ __forceinline__ int face_entry(int d, int x, int y, int z) {
-  return (d == PX || d == MX) ? y + 8 * z : (d == PY || d == MY) ? x + 8 * z : x + 8 * y;
-}
+
 
 // halo heights of tile t into sh (INF outside the grid): 384 entries, 12 per lane
 __device__ __forceinline__ void warp_load_halo_heights(const DevPool& P, int t, int* sh, int lane) {
