@@ -271,11 +271,17 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
       }
       int hnew = h;
       if (e > 0 && h < INF) {
+        // the labels of the pulse start, read again from S.h[cur] (the new
+        // ones go to the other buffer) rather than kept in registers
         bool adm = (rT > 0 && h == 1);
         int mn = (rT > 0) ? 0 : INF;
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
-          if (r[d] > 0) { adm = adm || (hn[d] == h - 1); mn = min(mn, hn[d]); }
+          if (r[d] > 0) {
+            const int hd = S.h[cur][hi + hoff(d)];
+            adm = adm || (hd == h - 1);
+            mn = min(mn, hd);
+          }
         }
         if (!adm) {
           hnew = (mn >= INF) ? INF : mn + 1;
