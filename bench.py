@@ -249,9 +249,9 @@ def main():
     B = Batch([(v.X, v.Y, v.Z)])
     B.bind_inputs(0, d_in[0].data_ptr(), d_in[1].data_ptr(), [t.data_ptr() for t in d_in[2:]])
     B.bind_outputs(0, d_seg[0].data_ptr(), d_seg[1].data_ptr())
-    cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr)
+    cands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr, bfs_warp_min=bw)
              for (L, R, K) in ((4, 2, 8), (2, 4, 4), (8, 2, 8), (4, 2, 16), (2, 4, 8), (4, 4, 8))
-             for c in (2, 3, 4) for lr in ((0, 1) if have_learned else (0,))]
+             for c in (2, 3, 4) for lr in ((0, 1) if have_learned else (0,)) for bw in ((0, 8) if c > 2 else (0,))]
     if args.schedule:
         L, R, K, c, lr = (int(x) for x in args.schedule.split(","))
         best, best_ms = Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, learned=lr), None
@@ -433,8 +433,9 @@ def main():
         for i, (d, o) in enumerate(zip(dins, douts)):
             BB.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
             BB.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
-        bcands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c)
-                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8)) for c in (2, 3, 4)]
+        bcands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, bfs_warp_min=bw)
+                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8)) for c in (2, 3, 4)
+                  for bw in ((0, 8) if c > 2 else (0,))]
         bbest, _ = BB.autotune(bcands, repeats=1)
 
         def time_batch(pol, reps=3):

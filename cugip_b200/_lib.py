@@ -37,7 +37,7 @@ class Options(C.Structure):
                 ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
                 ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("learned", C.c_int32), ("trace_cycles", C.c_int32),
-                ("warp_tiles", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("warp_tiles", C.c_int32), ("bfs_warp_min", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Stats(C.Structure):
@@ -156,7 +156,7 @@ def check(rc: int) -> None:
 
 def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
             persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0, ctas_per_sm: int = 0,
-            learned: int = 0, trace_cycles: int = 0, warp_tiles: int = 0) -> Options:
+            learned: int = 0, trace_cycles: int = 0, warp_tiles: int = 0, bfs_warp_min: int = 0) -> Options:
     o = Options()
     o.struct_size = C.sizeof(Options)
     o.local_pulses = local_pulses
@@ -170,4 +170,5 @@ def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 
     o.learned = learned
     o.trace_cycles = trace_cycles
     o.warp_tiles = warp_tiles
+    o.bfs_warp_min = bfs_warp_min
     return o

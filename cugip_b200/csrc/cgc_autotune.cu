@@ -46,16 +46,17 @@ void load_cache_locked() {
   if (!path) return;
   FILE* f = std::fopen(path, "r");
   if (!f) return;
-  // line: size class (2), L R K ctas stall warp, milliseconds
+  // line: size class (2), L R K ctas stall warp bfs_warp_min, milliseconds
   char line[256];
   while (std::fgets(line, sizeof line, f)) {
-    int ib, vb, L, R, K, cta, st, warp;
+    int ib, vb, L, R, K, cta, st, warp, bw;
     double ms;
-    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &warp, &ms) != 9) continue;
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &warp, &bw, &ms) != 10) continue;
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
     o.local_pulses = L; o.region_relabels = R; o.sweeps_per_relabel = K; o.ctas_per_sm = cta; o.stall_sweeps = st;
     o.warp_tiles = warp;
+    o.bfs_warp_min = bw;
     g_cache[{ib, vb}] = {o, ms};
   }
   std::fclose(f);
@@ -67,8 +68,8 @@ void store(std::pair<int, int> key, const cgc_options& o, double ms) {
   g_cache[key] = {o, ms};
   if (const char* path = std::getenv("CGC_AUTOTUNE_CACHE")) {
     if (FILE* f = std::fopen(path, "a")) {
-      std::fprintf(f, "%d %d %d %d %d %d %d %d %.6f\n", key.first, key.second, o.local_pulses, o.region_relabels,
-                   o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.warp_tiles, ms);
+      std::fprintf(f, "%d %d %d %d %d %d %d %d %d %.6f\n", key.first, key.second, o.local_pulses, o.region_relabels,
+                   o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.warp_tiles, o.bfs_warp_min, ms);
       std::fclose(f);
     }
   }
@@ -81,12 +82,15 @@ std::vector<cgc_options> default_candidates() {
   for (int cta : {2, 3, 4})
     for (int R : {1, 2, 4})
       for (int L : {2, 4, 8})
-        for (int K : {4, 8, 16}) {
-          cgc_options o{};
-          o.struct_size = sizeof(cgc_options);
-          o.local_pulses = L; o.region_relabels = R; o.sweeps_per_relabel = K; o.ctas_per_sm = cta;
-          c.push_back(o);
-        }
+        for (int K : {4, 8, 16})
+          for (int bw : {0, 8}) {
+            if (bw && cta == 2) continue;  // warp-per-tile BFS rounds exist at 3 and 4 CTAs/SM
+            cgc_options o{};
+            o.struct_size = sizeof(cgc_options);
+            o.local_pulses = L; o.region_relabels = R; o.sweeps_per_relabel = K; o.ctas_per_sm = cta;
+            o.bfs_warp_min = bw;
+            c.push_back(o);
+          }
   return c;
 }
 

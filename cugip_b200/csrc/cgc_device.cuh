@@ -125,6 +125,7 @@ struct SolveParams {
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
   int async = 0;         // 1: work-queue schedule (CGC_SCHED_ASYNC)
+  int bfs_warp_min = 0;  // BFS rounds with at least this many tiles per CTA run a warp per tile (0: never)
 };
 
 // kernels of cgc_engine.cu launched from other translation units
@@ -135,6 +136,8 @@ __global__ void k_prepare(DevPool P);
 __global__ void k_solve(DevPool P, SolveParams prm);
 __global__ void k_solve3(DevPool P, SolveParams prm);
 __global__ void k_solve4(DevPool P, SolveParams prm);
+__global__ void k_solve3w(DevPool P, SolveParams prm);
+__global__ void k_solve4w(DevPool P, SolveParams prm);
 __global__ void k_solve_q(DevPool P, SolveParams prm);
 __global__ void k_solve_q3(DevPool P, SolveParams prm);
 constexpr int WARP_CTA_WARPS = 10;  // warps of the warp-per-tile solve CTA (one CTA per SM)

@@ -254,9 +254,14 @@ __device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams&
   return true;
 }
 
+// BFS rounds with many tiles run a warp per tile on the first BFS_WARPS warps
+// of each CTA (one WarpBfsSmem slice each).
+constexpr int BFS_WARPS = 8;
+
 union SolveShared {
   SweepShared sw;
   BfsShared bfs;
+  WarpBfsSmem wbfs[BFS_WARPS];
   ReachShared rc;
   SchedShared sched;
 };
@@ -264,7 +269,7 @@ union SolveShared {
 // The whole solve in one cooperative launch.  WARP = false: a CTA of 512
 // threads is the unit that visits a tile (SolveShared); WARP = true: every
 // warp of the CTA visits tiles on its own (WarpSmem per warp).
-template <bool WARP>
+template <bool WARP, bool BFSW = false>
 __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, void* smem) {
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   SolveShared& S = *reinterpret_cast<SolveShared*>(smem);
@@ -346,10 +351,29 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const int n = ld_cnt(bc + k % 3);
       if (n == 0) break;
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-      for_entries(n, [&](int i) {
-        if constexpr (WARP) bfs_tile_w(P, __ldcg(bl[k % 3] + i), W.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-        else bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-      });
+      if (BFSW && !WARP && n / G >= prm.bfs_warp_min) {
+        // Throughput-bound round: a warp per tile (no block barriers, a
+        // tile's relaxation costs one warp's issue slots instead of 16),
+        // entries handed out like for_entries, per warp.
+        int32_t* take = P.cnt + C_TAKE0 + round_no % 3;
+        if (b == 0 && tid == 0) P.cnt[C_TAKE0 + (round_no + 1) % 3] = 0;
+        ++round_no;
+        const int wid = tid >> 5;
+        if (wid < BFS_WARPS) {
+          int i = b * BFS_WARPS + wid;
+          while (i < n) {
+            int nx = 0;
+            if ((tid & 31) == 0) nx = atomicAdd(take, 1);
+            bfs_tile_w(P, __ldcg(bl[k % 3] + i), S.wbfs[wid], bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+            i = G * BFS_WARPS + __shfl_sync(0xffffffffu, nx, 0);
+          }
+        }
+      } else {
+        for_entries(n, [&](int i) {
+          if constexpr (WARP) bfs_tile_w(P, __ldcg(bl[k % 3] + i), W.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+          else bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+        });
+      }
       ++k;
       if (!grid_sync(P, prm.limit_ns)) return;
       record(TR_BFS_ROUND, rounds + k, n);
@@ -658,8 +682,9 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
       if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q3, d, prm));
       else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q, d, prm));
     } else {
-      if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve4, d, prm));
-      else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve3, d, prm));
+      const bool bw = prm.bfs_warp_min > 0;
+      if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve4w : k_solve4, d, prm));
+      else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve3w : k_solve3, d, prm));
       else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
     }
   }
@@ -679,6 +704,16 @@ __global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
 __global__ void __launch_bounds__(512, 4) k_solve4(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
   solve_body<false>(P, prm, &S);
+}
+// The same with warp-per-tile BFS rounds (SolveParams::bfs_warp_min); separate
+// kernels, so that the others do not carry that code's registers.
+__global__ void __launch_bounds__(512, 3) k_solve3w(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_body<false, true>(P, prm, &S);
+}
+__global__ void __launch_bounds__(512, 4) k_solve4w(DevPool P, SolveParams prm) {
+  __shared__ SolveShared S;
+  solve_body<false, true>(P, prm, &S);
 }
 // The solve under the work-queue schedule, at 2 and 3 CTAs per SM.
 __global__ void __launch_bounds__(512, 2) k_solve_q(DevPool P, SolveParams prm) {
@@ -845,9 +880,12 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   int occ3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_solve3, 512, 0));
   p->coop_blocks3 = std::max(1, occ3) * p->sms;
-  int occ4 = 0;
+  int occ4 = 0, occ3w = 0, occ4w = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4, k_solve4, 512, 0));
-  p->coop_blocks4 = std::max(1, occ4) * p->sms;
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3w, k_solve3w, 512, 0));
+  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4w, k_solve4w, 512, 0));
+  p->coop_blocks4 = std::max(1, std::min(occ4, occ4w)) * p->sms;
+  p->coop_blocks3 = std::min(p->coop_blocks3, std::max(1, occ3w) * p->sms);
   // the work-queue kernels have the same launch bounds; take the smaller grid
   int occq = 0, occq3 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, k_solve_q, 512, 0));
@@ -926,6 +964,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
     if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
     r.warp_tiles = o->warp_tiles > 0 ? 1 : 0;
+    r.bfs_warp_min = o->bfs_warp_min > 0 ? o->bfs_warp_min : 0;
     r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
@@ -1006,6 +1045,7 @@ int pool_solve(Pool& p, const cgc_options* opts) {
     prm.max_sweeps = (int64_t)o.max_sweeps;
     prm.limit_ns = 20ull * 1000000000ull;
     prm.async = o.schedule == CGC_SCHED_ASYNC ? 1 : 0;
+    prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
     CGC_CUDA(cudaEventRecord(evk0, p.stream));
     rc = launch_solve(p, o, d, prm, p.stream);
     if (rc) { destroy_events(); return rc; }

@@ -83,7 +83,9 @@ typedef struct cgc_options {
   int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
   int32_t warp_tiles;         /* persistent: 1 = one warp per tile visit (ten warps per SM), 0 = one 512-thread CTA */
-  int32_t reserved[4];
+  int32_t bfs_warp_min;       /* persistent, 3 or 4 CTAs/SM: BFS rounds with at least this many tiles per CTA
+                                 visit a tile with one warp (0 = never, the default) */
+  int32_t reserved[3];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */

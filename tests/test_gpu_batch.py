@@ -53,7 +53,8 @@ def test_enqueue_matches_golden(device_batch):
 
 
 @pytest.mark.parametrize("policy", [Policy(), Policy(local_pulses=2, region_relabels=4, sweeps_per_relabel=4, ctas_per_sm=3),
-                                    Policy(warp_tiles=1), Policy(schedule=1), Policy(ctas_per_sm=4, region_relabels=4)])
+                                    Policy(warp_tiles=1), Policy(schedule=1), Policy(ctas_per_sm=4, region_relabels=4),
+                                    Policy(ctas_per_sm=4, region_relabels=4, bfs_warp_min=8)])
 def test_graph_replay_matches_golden(device_batch, policy):
     B, vols, ins, outs, flows = device_batch
     B.graph_create(policy, flows.data_ptr())

@@ -30,6 +30,8 @@ POLICIES = {
     "stall1_K64": Policy(stall_sweeps=1, sweeps_per_relabel=64),
     "stall3_L2": Policy(stall_sweeps=3, local_pulses=2, sweeps_per_relabel=16),
     "cta4_R4": Policy(ctas_per_sm=4, region_relabels=4),
+    "bfsw_all": Policy(ctas_per_sm=3, bfs_warp_min=1),
+    "bfsw8_cta4": Policy(ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
     "warp": Policy(warp_tiles=1),
     "warp_L1_K1": Policy(warp_tiles=1, local_pulses=1, sweeps_per_relabel=1),
     "warp_no_region": Policy(warp_tiles=1, region_relabels=-1, local_pulses=8),
@@ -96,7 +98,7 @@ def test_long_paths_match_oracle(seed):
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "cta4_R4", "warp", "async"])
+@pytest.mark.parametrize("policy", ["default", "cta4_R4", "bfsw_all", "bfsw8_cta4", "warp", "async"])
 @pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 4, 5)])
 def test_golden_workloads(key, policy):
     c = CASES[key]
@@ -108,7 +110,7 @@ def test_golden_workloads(key, policy):
     assert sha(treach) == c["treach_sha256"]
 
 
-@pytest.mark.parametrize("policy", ["default", "warp", "async"])
+@pytest.mark.parametrize("policy", ["default", "bfsw8_cta4", "warp", "async"])
 @pytest.mark.parametrize("key", [(2, 0), (3, 0)])
 def test_full_size_workloads_with_certificate(key, policy):
     c = CASES[key]
@@ -227,7 +229,7 @@ def test_sparse_terminals_match_oracle(seed, policy):
 
 
 @pytest.mark.parametrize("policy", ["default", "host_loop", "no_region", "warp", "warp_no_region", "async",
-                                    "async_no_region"])
+                                    "async_no_region", "bfsw_all"])
 @pytest.mark.parametrize("axis,n", [(0, 2), (0, 9), (0, 16), (0, 40), (1, 17), (2, 24), (0, 64)])
 def test_chain_through_every_voxel(axis, n, policy):
     """A 1-D chain with the source at one end and the sink at the other: the
