@@ -334,3 +334,69 @@ def test_scheduling_traces_are_recorded():
     assert active.any()
     assert (pulses[active] > 0).all()          # every active tile was visited
     assert not (f[~active] != 0).any()         # inactive tiles have zero features
+
+
+def _device_cut_capacity(capS, capT, fwd, bwd, side):
+    """Capacity of the cut (side = source set) on the device, in int64, one z
+    slice of the (Z, Y, X) volumes at a time: capT over the source side, capS
+    over the rest, n-links from the source side to the rest."""
+    import torch
+    Z = side.shape[0]
+    total = 0
+    for z in range(Z):
+        s = side[z].bool()
+        total += int(capT[z][s].sum(dtype=torch.int64)) + int(capS[z][~s].sum(dtype=torch.int64))
+        # x and y links inside the slice: v -> v+e with fwd[v], v+e -> v with bwd[v]
+        for ax, (f, b) in enumerate(((fwd[0][z], bwd[0][z]), (fwd[1][z], bwd[1][z]))):
+            if ax == 0:
+                a, c, fa, ba = s[:, :-1], s[:, 1:], f[:, :-1], b[:, :-1]
+            else:
+                a, c, fa, ba = s[:-1, :], s[1:, :], f[:-1, :], b[:-1, :]
+            total += int(fa[a & ~c].sum(dtype=torch.int64)) + int(ba[~a & c].sum(dtype=torch.int64))
+        if z + 1 < Z:
+            c = side[z + 1].bool()
+            total += int(fwd[2][z][s & ~c].sum(dtype=torch.int64)) + int(bwd[2][z][~s & c].sum(dtype=torch.int64))
+    return total
+
+
+def test_largest_grid_certificate():
+    """768^3 (453 M voxels; the residual planes span more than 2^31 entries):
+    random capacities made on the device, solved through the device API; both
+    returned cuts -- the minimal source side and the complement of the sink
+    side -- have a capacity equal to the flow, which certifies a maximum flow
+    and a minimum cut without a CPU solve."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n = 768
+    if torch.cuda.get_device_properties(0).total_memory < 80 * 2 ** 30:
+        pytest.skip("needs a GPU with 80 GB or more")
+    g = torch.Generator(device=dev)
+    g.manual_seed(768)
+
+    def plane(hi, zero_frac):
+        p = torch.randint(0, hi, (n, n, n), generator=g, device=dev, dtype=torch.int32)
+        p[torch.rand((n, n, n), generator=g, device=dev) < zero_frac] = 0
+        return p
+
+    capS, capT = plane(60, 0.7), plane(60, 0.7)
+    fwd = [plane(40, 0.2) for _ in range(3)]
+    # no capacity leaves the grid
+    fwd[0][:, :, -1] = 0
+    fwd[1][:, -1, :] = 0
+    fwd[2][-1, :, :] = 0
+    G = GridGraph(n, n, n)
+    try:
+        G.set_tweights_device(capS.data_ptr(), capT.data_ptr())
+        for ax in range(3):
+            G.set_nweights_device(ax, fwd[ax].data_ptr())
+        flow = G.max_flow()
+        smin = torch.empty((n, n, n), dtype=torch.uint8, device=dev)
+        treach = torch.empty((n, n, n), dtype=torch.uint8, device=dev)
+        G.fill_segments_device(smin.data_ptr(), 1, 0, SOURCE)
+        G.fill_segments_device(treach.data_ptr(), 1, 0, SINK)
+    finally:
+        G.close()
+    assert flow > 0
+    assert not bool((smin.bool() & treach.bool()).any())  # a source-side voxel cannot reach the sink
+    assert _device_cut_capacity(capS, capT, fwd, fwd, smin) == flow
+    assert _device_cut_capacity(capS, capT, fwd, fwd, 1 - treach) == flow
