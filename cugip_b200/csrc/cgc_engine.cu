@@ -904,18 +904,57 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   return ok();
 }
 
+// Host upload of one or two planes into the next of the two staging buffers,
+// on a copy stream of its own.  Returns once the host arrays have been read,
+// which is the setters' contract (the caller may reuse them at once, pinned or
+// not).  The permute kernel that follows runs on the solve stream while the
+// next upload already copies into the other buffer; a buffer is overwritten
+// only after the kernel that read it (event `consumed`, recorded by
+// stage_done).
+static int stage_upload(Pool& p, const int32_t* a, const int32_t* b, int64_t N, const int32_t** da,
+                        const int32_t** db) {
+  if (!p.copy_stream) {
+    CGC_CUDA(cudaStreamCreateWithFlags(&p.copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      CGC_CUDA(cudaEventCreateWithFlags(&p.staged[k], cudaEventDisableTiming));
+      CGC_CUDA(cudaEventCreateWithFlags(&p.consumed[k], cudaEventDisableTiming));
+    }
+    CGC_CUDA(cudaMalloc(&p.staging2, 2 * p.maxN * 4));
+  }
+  const int k = p.stage;
+  int32_t* buf = k ? p.staging2 : p.staging;
+  CGC_CUDA(cudaStreamWaitEvent(p.copy_stream, p.consumed[k], 0));  // no-op before the first record
+  CGC_CUDA(cudaMemcpyAsync(buf, a, N * 4, cudaMemcpyHostToDevice, p.copy_stream));
+  if (b) CGC_CUDA(cudaMemcpyAsync(buf + p.maxN, b, N * 4, cudaMemcpyHostToDevice, p.copy_stream));
+  CGC_CUDA(cudaEventRecord(p.staged[k], p.copy_stream));
+  CGC_CUDA(cudaEventSynchronize(p.staged[k]));
+  *da = buf;
+  if (db) *db = b ? buf + p.maxN : nullptr;
+  return CGC_OK;
+}
+
+// After the kernel that reads the current staging buffer was launched.
+static int stage_done(Pool& p) {
+  CGC_CUDA(cudaEventRecord(p.consumed[p.stage], p.stream));
+  p.stage ^= 1;
+  return CGC_OK;
+}
+
 int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host) {
   if (inst < 0 || inst >= p.ninst || !capS || !capT) return fail(CGC_ERR_ARG, "set_tlinks: bad arguments");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
   const int32_t *s = capS, *c = capT;
   if (host) {
-    CGC_CUDA(cudaMemcpyAsync(p.staging, capS, N * 4, cudaMemcpyHostToDevice, p.stream));
-    CGC_CUDA(cudaMemcpyAsync(p.staging + p.maxN, capT, N * 4, cudaMemcpyHostToDevice, p.stream));
-    s = p.staging; c = p.staging + p.maxN;
+    int rc = stage_upload(p, capS, capT, N, &s, &c);
+    if (rc) return rc;
   }
   k_put_tlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, s, c); note_launch();
   CGC_CUDA(cudaGetLastError());
+  if (host) {
+    int rc = stage_done(p);
+    if (rc) return rc;
+  }
   p.uploaded[inst] |= 1u;
   p.solved = false;
   return ok();
@@ -928,16 +967,17 @@ int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
   const int32_t *f = fwd, *b = bwd;
   if (host) {
-    CGC_CUDA(cudaMemcpyAsync(p.staging, fwd, N * 4, cudaMemcpyHostToDevice, p.stream));
-    f = p.staging;
-    if (bwd == fwd) b = p.staging;
-    else {
-      CGC_CUDA(cudaMemcpyAsync(p.staging + p.maxN, bwd, N * 4, cudaMemcpyHostToDevice, p.stream));
-      b = p.staging + p.maxN;
-    }
+    const bool same = bwd == fwd;  // symmetric weights: one plane
+    int rc = stage_upload(p, fwd, same ? nullptr : bwd, N, &f, &b);
+    if (rc) return rc;
+    if (same) b = f;
   }
   k_put_nlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, axis, f, b); note_launch();
   CGC_CUDA(cudaGetLastError());
+  if (host) {
+    int rc = stage_done(p);
+    if (rc) return rc;
+  }
   p.uploaded[inst] |= 2u << axis;
   p.solved = false;
   return ok();

@@ -36,6 +36,13 @@ struct Pool {
   DevPool dp{};
   void* dbuf = nullptr;          // all device state
   int32_t* staging = nullptr;    // 2*maxN int32
+  // host uploads alternate between staging and staging2 on copy_stream
+  // (stage_upload in cgc_engine.cu); created on the first host upload
+  int32_t* staging2 = nullptr;   // 2*maxN int32
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t staged[2] = {nullptr, nullptr};    // the copy into buffer k has finished
+  cudaEvent_t consumed[2] = {nullptr, nullptr};  // the kernel reading buffer k has finished
+  int stage = 0;
   uint8_t* seg = nullptr;        // maxN bytes
   int32_t* pinned_cnt = nullptr; // host-pinned counters
   bool solved = false;
@@ -72,6 +79,12 @@ struct Pool {
     if (d_out) cudaFree(d_out);
     if (dbuf) cudaFree(dbuf);
     if (staging) cudaFree(staging);
+    if (staging2) cudaFree(staging2);
+    for (int k = 0; k < 2; ++k) {
+      if (staged[k]) cudaEventDestroy(staged[k]);
+      if (consumed[k]) cudaEventDestroy(consumed[k]);
+    }
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (seg) cudaFree(seg);
     if (pinned_cnt) cudaFreeHost(pinned_cnt);
   }

@@ -400,3 +400,32 @@ def test_largest_grid_certificate():
     assert not bool((smin.bool() & treach.bool()).any())  # a source-side voxel cannot reach the sink
     assert _device_cut_capacity(capS, capT, fwd, fwd, smin) == flow
     assert _device_cut_capacity(capS, capT, fwd, fwd, 1 - treach) == flow
+
+
+def test_host_setters_copy_before_returning():
+    """The setters' contract (the reference copies at call time): once a setter
+    returns, the caller may overwrite its arrays -- here pinned ones, whose
+    copies would otherwise still be in flight."""
+    import torch
+    X, Y, Z = 48, 40, 24
+    capS, capT, fwd, bwd = graphs.random_grid(X, Y, Z, 4242)
+    f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
+    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in (capS, capT, *fwd, *bwd)]
+    host = [t.numpy() for t in pin]
+    g = GridGraph(X, Y, Z)
+    try:
+        for rep in range(2):
+            for t, a in zip(pin, (capS, capT, *fwd, *bwd)):
+                t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+            g.set_tweights(host[0], host[1])
+            host[0][:] = 7777
+            host[1][:] = 0
+            for ax in range(3):
+                g.set_nweights(ax, host[2 + ax], host[5 + ax])
+                host[2 + ax][:] = 12345
+                host[5 + ax][:] = 0
+            assert g.max_flow() == f0
+            assert np.array_equal(g.fill_segments(mask=1, which=SOURCE), s0)
+            assert np.array_equal(g.fill_segments(mask=1, which=SINK), t0)
+    finally:
+        g.close()
