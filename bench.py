@@ -74,6 +74,38 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
+def generic_layered() -> dict:
+    """The generic (non-grid) engine on the layered graph of the reference's
+    unit_tests/graph_cut_test.cu:22-65 (100 layers of 1024 vertices, 8
+    neighbours in the next layer, a 1 / 2 bottleneck in the middle layer,
+    terminals of 100000 on the first and last layer; known flow 1024 * 8)."""
+    import numpy as np
+    from cugip_b200.graph_cut import GenericGraph
+    layers, size, nbrs = 100, 1024, 8
+    i = np.arange(size)
+    a, b, f = [], [], []
+    for layer in range(1, layers):
+        w = 1 if layer == layers // 2 else 20
+        for j in range(nbrs):
+            a.append((layer - 1) * size + i)
+            b.append(layer * size + (i + j) % size)
+            f.append(np.full(size, w))
+    a, b, f = np.concatenate(a), np.concatenate(b), np.concatenate(f)
+    n = layers * size
+    src, snk = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    src[:size] = 100000
+    snk[-size:] = 100000
+    with GenericGraph(n, a, b, f, 2 * f) as g:
+        g.set_tweights(src, snk)
+        runs = []
+        for _ in range(4):
+            flow = g.max_flow()
+            runs.append(g.stats()["kernel_ms"])
+        if flow != 1024 * 8:
+            raise SystemExit(f"generic engine: layered flow {flow}, expected {1024 * 8}")
+    return {"ms": min(runs[1:]), "vertices": n, "edges": int(a.size), "flow": flow}
+
+
 def profiled_traffic(workload: int):
     """dram bytes per k_solve launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"k_solve_workload{workload}_traffic.txt")
@@ -466,6 +498,7 @@ def main():
         var["batch96_speedup_batched_vs_plain"] = seq_ms / bat_ms
         var["batch96_voxels"] = tot
         BB.close()
+        var["generic_layered"] = generic_layered()
         line["variants"] = var
 
     if rank == 0:
