@@ -74,6 +74,45 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
+def learned_report(workloads=(1, 3)) -> dict:
+    """The learned scheduler against the same fixed schedule without it, on the
+    64^3 two-sphere and 512x512x128 tube workloads: kernel time, exact global
+    relabels (saved = plain - learned) and bit-identity of the flow and of
+    both cut sets."""
+    import hashlib
+    import numpy as np
+    import torch
+    from cugip_b200 import volume
+    from cugip_b200.graph_cut import SINK, SOURCE, GridGraph, Policy
+    out = {}
+    for w in workloads:
+        v = volume.workload(w)
+        d = [torch.from_numpy(a).cuda() for a in v.arrays()]
+        g = GridGraph(v.X, v.Y, v.Z)
+        res = {}
+        try:
+            for name, pol in (("plain", Policy(local_pulses=4, region_relabels=2, sweeps_per_relabel=8, ctas_per_sm=3)),
+                              ("learned", Policy(local_pulses=4, region_relabels=2, sweeps_per_relabel=8, ctas_per_sm=3,
+                                                 learned=1))):
+                runs = []
+                for _ in range(3):
+                    g.set_tweights_device(d[0].data_ptr(), d[1].data_ptr())
+                    for ax in range(3):
+                        g.set_nweights_device(ax, d[2 + ax].data_ptr())
+                    flow = g.max_flow(pol)
+                    runs.append(g.stats())
+                cuts = [hashlib.sha256(g.fill_segments(mask=1, which=k).tobytes()).hexdigest() for k in (SOURCE, SINK)]
+                best = min(runs, key=lambda s: s["kernel_ms"])
+                res[name] = (flow, cuts, best["kernel_ms"], int(best["global_relabels"]))
+        finally:
+            g.close()
+        (fp, cp, mp, rp), (fl, cl, ml, rl) = res["plain"], res["learned"]
+        out[f"workload{w}"] = {"voxels": v.N, "plain_ms": mp, "learned_ms": ml, "speedup": mp / ml,
+                               "relabels_plain": rp, "relabels_learned": rl, "relabels_saved": rp - rl,
+                               "bit_identical": fp == fl and cp == cl}
+    return out
+
+
 def generic_layered() -> dict:
     """The generic (non-grid) engine on the layered graph of the reference's
     unit_tests/graph_cut_test.cu:22-65 (100 layers of 1024 vertices, 8
@@ -499,6 +538,8 @@ def main():
         var["batch96_voxels"] = tot
         BB.close()
         var["generic_layered"] = generic_layered()
+        if have_learned:
+            var["learned_config5"] = learned_report()
         line["variants"] = var
 
     if rank == 0:
