@@ -54,6 +54,13 @@ struct GraphCutPolicy {
   int region_relabels = 0;     // region relabels per tile visit (-1: none)
   int sweeps_per_relabel = 0;  // sweep pairs between exact global relabels
   int persistent = 0;          // 1: one cooperative launch, -1: host loop
+  int schedule = 0;            // CGC_SCHED_PARITY (default) or CGC_SCHED_ASYNC
+  int max_sweeps = 0;          // safety cap (0: default)
+  int stall_sweeps = 0;        // relabel early after this many idle sweep pairs (0: never)
+  int ctas_per_sm = 0;         // 2 (default), 3 or 4 CTAs per SM
+  int learned = 0;             // learned scheduler: 1 budgets + priorities, 2 budgets only
+  int warp_tiles = 0;          // 1: one warp per tile visit
+  int bfs_warp_min = 0;        // 3/4 CTAs per SM: BFS rounds with this many tiles per CTA use a warp per tile
   cgc_options options() const {
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
@@ -61,13 +68,40 @@ struct GraphCutPolicy {
     o.region_relabels = region_relabels;
     o.sweeps_per_relabel = sweeps_per_relabel;
     o.persistent = persistent;
+    o.schedule = schedule;
+    o.max_sweeps = max_sweeps;
+    o.stall_sweeps = stall_sweeps;
+    o.ctas_per_sm = ctas_per_sm;
+    o.learned = learned;
+    o.warp_tiles = warp_tiles;
+    o.bfs_warp_min = bfs_warp_min;
     return o;
+  }
+  // The autotuner's choice for a size class (cgc_autotune_lookup), if any
+  // solve of that class was tuned in this process or is in the cache file.
+  static bool autotuned(int64_t voxels, int32_t instances, GraphCutPolicy* out) {
+    cgc_options o{};
+    o.struct_size = sizeof(cgc_options);
+    if (cgc_autotune_lookup(voxels, instances, &o) != CGC_OK) return false;
+    out->local_pulses = o.local_pulses;
+    out->region_relabels = o.region_relabels;
+    out->sweeps_per_relabel = o.sweeps_per_relabel;
+    out->persistent = o.persistent;
+    out->schedule = o.schedule;
+    out->max_sweeps = o.max_sweeps;
+    out->stall_sweeps = o.stall_sweeps;
+    out->ctas_per_sm = o.ctas_per_sm;
+    out->learned = o.learned;
+    out->warp_tiles = o.warp_tiles;
+    out->bfs_warp_min = o.bfs_warp_min;
+    return true;
   }
 };
 
 // Trace protocol of the reference.  The solve runs as one device launch, so
-// the per-iteration hooks are replayed after it with the solve statistics
-// (one iteration per exact global relabel).
+// the per-iteration hooks are replayed after it: one iteration per exact
+// global relabel, with the level starts of that relabel's BFS rounds from the
+// solve's phase trace.
 struct DummyTraceObject {
   void computationStarted(const cgc_stats&) {}
   void beginIteration(int) {}

@@ -120,6 +120,34 @@ int main() {
   g.set_tweights(cs.data(), ct.data());
   g.set_nweights(CGC_AXIS_X, nx.data(), nx.data());
   EXPECT(g.max_flow() == 3);
+  // every kernel shape a policy selects gives the same flow on a 48^3 grid
+  // with pseudo-random weights
+  {
+    const int X = 48, Y = 48, Z = 48, N = X * Y * Z;
+    std::vector<int32_t> s(N), t(N), ax[3];
+    unsigned v = 12345u;
+    auto rnd = [&v](int m) { v = v * 1664525u + 1013904223u; return (int32_t)((v >> 8) % (unsigned)m); };
+    for (int i = 0; i < N; ++i) { s[i] = rnd(100) < 30 ? rnd(40) : 0; t[i] = rnd(100) < 30 ? rnd(40) : 0; }
+    for (auto& a : ax) { a.resize(N); for (auto& c : a) c = rnd(25); }
+    cgc::GridGraph grid(X, Y, Z);
+    auto solve = [&](const cgc::GraphCutPolicy* p) {
+      grid.set_tweights(s.data(), t.data());
+      for (int k = 0; k < 3; ++k) grid.set_nweights(k, ax[k].data(), ax[k].data());
+      return grid.max_flow(p);
+    };
+    const int64_t f0 = solve(nullptr);
+    EXPECT(f0 > 0);
+    cgc::GraphCutPolicy pols[6];
+    pols[0].ctas_per_sm = 3; pols[0].bfs_warp_min = 1;
+    pols[1].ctas_per_sm = 4; pols[1].region_relabels = 4; pols[1].local_pulses = 2;
+    pols[2].schedule = CGC_SCHED_ASYNC;
+    pols[3].warp_tiles = 1;
+    pols[4].persistent = -1; pols[4].sweeps_per_relabel = 4;
+    pols[5].stall_sweeps = 2; pols[5].ctas_per_sm = 3;
+    for (const auto& p : pols) EXPECT(solve(&p) == f0);
+    cgc::GraphCutPolicy tuned;
+    EXPECT(!cgc::GraphCutPolicy::autotuned((int64_t)N * 7 + 1, 1, &tuned));
+  }
   std::printf("cpp facade ok\n");
   return 0;
 }
