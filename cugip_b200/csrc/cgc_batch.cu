@@ -26,85 +26,147 @@ namespace cgc {
 // (the capacity into the voxel from each neighbour: bwd[v] from +a,
 // fwd[v - stride] from -a) is an input this thread reads anyway, so the solve
 // starts after one pass over the planes instead of two.
-__global__ void __launch_bounds__(512) k_put_all(DevPool P, const int32_t* const* __restrict__ in) {
-  __shared__ long long red[16];
+//
+// One CTA of 128 threads per tile; thread q owns the four voxels 4q..4q+3 of
+// the tile (four consecutive x of one row).  The kernel is bound by load
+// latency, so every load of a thread is issued unconditionally and at once:
+// indices outside the instance are clamped to a valid voxel and missing
+// planes read capS, and the values are masked afterwards.  The outputs are
+// 16-byte stores into the tile-blocked planes.
+__global__ void __launch_bounds__(128) k_put_all(DevPool P, const int32_t* const* __restrict__ in) {
+  __shared__ long long red[4];
   const int t = blockIdx.x;
   const int inst = P.tinst[t];
   const InstGeo G = P.geo[inst];
   const int lt = t - G.tile_base;
   const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
-  const int l = threadIdx.x;
-  const int x = tx * 8 + (l & 7), y = ty * 8 + ((l >> 3) & 7), z = tz * 8 + (l >> 6);
-  const int64_t g = (int64_t)t * TV + l;
+  const int q = threadIdx.x, l0 = 4 * q;
+  const int x0 = tx * 8 + (l0 & 7), y = ty * 8 + ((l0 >> 3) & 7), z = tz * 8 + (l0 >> 6);
+  const int64_t g0 = (int64_t)t * TV + l0;
   const int32_t* const* ip = in + 8 * inst;
-  int s = 0, c = 0, r[6] = {0, 0, 0, 0, 0, 0}, back[6] = {0, 0, 0, 0, 0, 0};
-  if (x < G.X && y < G.Y && z < G.Z) {
-    const int64_t v = x + (int64_t)G.X * (y + (int64_t)G.Y * z);
-    s = ip[0][v];
-    c = ip[1][v];
-    const int co[3] = {x, y, z}, ex[3] = {G.X, G.Y, G.Z};
-    const int64_t st[3] = {1, (int64_t)G.X, (int64_t)G.X * G.Y};
+  const int32_t* cs = ip[0];
+  const int32_t* ct = ip[1];
+  const int32_t* fp[3];
+  const int32_t* bp[3];
+  bool hasf[3], hasb[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    fp[a] = ip[2 + a]; bp[a] = ip[5 + a];
+    hasf[a] = fp[a] != nullptr; hasb[a] = bp[a] != nullptr;
+    if (!hasf[a]) fp[a] = cs;  // read something valid, then mask
+    if (!hasb[a]) bp[a] = cs;
+  }
+  // vrow: the thread's first voxel, or voxel 0 when that lies outside the instance
+  const bool row = y < G.Y && z < G.Z && x0 < G.X;
+  const int64_t vrow = row ? x0 + (int64_t)G.X * (y + (int64_t)G.Y * z) : 0;
+  const int ex[3] = {G.X, G.Y, G.Z};
+  const int64_t st[3] = {1, (int64_t)G.X, (int64_t)G.X * G.Y};
+  const int co[3] = {0, y, z};  // x is per voxel
+  // loads (all independent)
+  int s[4], c[4], fv[3][4], bv[3][4], fm[3][4], bm[3][4];
+  bool ok[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ok[k] = row && x0 + k < G.X;
+    const int64_t v = ok[k] ? vrow + k : vrow;
+    s[k] = cs[v];
+    c[k] = ct[v];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const int32_t* f = ip[2 + a];
-      const int32_t* b = ip[5 + a];
-      if (co[a] + 1 < ex[a]) {
-        if (f) r[2 * a] = f[v];          // v -> v + e_a
-        if (b) back[2 * a] = b[v];       // v + e_a -> v
-      }
-      if (co[a] > 0) {
-        if (b) r[2 * a + 1] = b[v - st[a]];      // v -> v - e_a
-        if (f) back[2 * a + 1] = f[v - st[a]];   // v - e_a -> v
-      }
+      const int cc = a == 0 ? x0 + k : co[a];
+      const int64_t vm = cc > 0 && ok[k] ? v - st[a] : v;
+      fv[a][k] = fp[a][v];
+      bv[a][k] = bp[a][v];
+      fm[a][k] = fp[a][vm];
+      bm[a][k] = bp[a][vm];
     }
-    bool neg = s < 0 || c < 0;
-#pragma unroll
-    for (int d = 0; d < 6; ++d) neg = neg || r[d] < 0;
-    if (neg) raise_error(P, CGC_ERR_ARG);
   }
+  int r[6][4];
+  long long inflow[4];
+  bool neg = false, bad = false;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    inflow[k] = 0;
+    if (!ok[k]) { s[k] = 0; c[k] = 0; }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int cc = a == 0 ? x0 + k : co[a];
+      const bool up = ok[k] && cc + 1 < ex[a], dn = ok[k] && cc > 0;
+      r[2 * a][k] = up && hasf[a] ? fv[a][k] : 0;        // v -> v + e_a
+      const int back_p = up && hasb[a] ? bv[a][k] : 0;   // v + e_a -> v
+      r[2 * a + 1][k] = dn && hasb[a] ? bm[a][k] : 0;    // v -> v - e_a
+      const int back_m = dn && hasf[a] ? fm[a][k] : 0;   // v - e_a -> v
+      inflow[k] += (long long)back_p + back_m;
+      bad = bad || (long long)r[2 * a][k] + back_p > 2147483647ll || (long long)r[2 * a + 1][k] + back_m > 2147483647ll;
+    }
+    neg = neg || s[k] < 0 || c[k] < 0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) neg = neg || r[d][k] < 0;
+  }
+  if (neg) raise_error(P, CGC_ERR_ARG);
   // t-link cancellation: min(capS, capT) flows straight through
-  const int mcap = min(s, c);
-  const int e = s - mcap, rT = c - mcap;
-  long long inflow = e;
-  bool bad = false;
-  unsigned m = (rT > 0 ? 64u : 0u) | (e > 0 ? 128u : 0u);
+  int e[4], rT[4];
+  unsigned m4 = 0;
+  long long tot = 0;
 #pragma unroll
-  for (int d = 0; d < 6; ++d) {
-    inflow += back[d];
-    if ((long long)r[d] + back[d] > 2147483647ll) bad = true;
-    m |= (r[d] > 0 ? 1u : 0u) << d;
+  for (int k = 0; k < 4; ++k) {
+    const int mcap = min(s[k], c[k]);
+    e[k] = s[k] - mcap;
+    rT[k] = c[k] - mcap;
+    tot += mcap;
+    unsigned m = (rT[k] > 0 ? 64u : 0u) | (e[k] > 0 ? 128u : 0u);
+#pragma unroll
+    for (int d = 0; d < 6; ++d) m |= (r[d][k] > 0 ? 1u : 0u) << d;
+    m4 |= m << (8 * k);
+    bad = bad || inflow[k] + e[k] > 2147483647ll;
   }
-  if (bad || inflow > 2147483647ll) raise_error(P, CGC_ERR_OVERFLOW);
-  P.e[g] = e;
-  P.rT[g] = rT;
+  if (bad) raise_error(P, CGC_ERR_OVERFLOW);
+  *reinterpret_cast<int4*>(P.e + g0) = make_int4(e[0], e[1], e[2], e[3]);
+  *reinterpret_cast<int4*>(P.rT + g0) = make_int4(rT[0], rT[1], rT[2], rT[3]);
 #pragma unroll
-  for (int d = 0; d < 6; ++d) P.r[d * P.Np + g] = r[d];
-  P.h[g] = 0;  // no label yet (INF would read as "dead" to the first global relabel)
-  P.rmask[g] = (uint8_t)m;
-  P.reach[g] = 0;
-  const long long tot = block_sum64((long long)mcap, red);
-  if (l == 0) {
+  for (int d = 0; d < 6; ++d)
+    *reinterpret_cast<int4*>(P.r + d * P.Np + g0) = make_int4(r[d][0], r[d][1], r[d][2], r[d][3]);
+  // no label yet (INF would read as "dead" to the first global relabel)
+  *reinterpret_cast<int4*>(P.h + g0) = make_int4(0, 0, 0, 0);
+  *reinterpret_cast<uint32_t*>(P.rmask + g0) = m4;
+  *reinterpret_cast<uint32_t*>(P.reach + g0) = 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+  if ((q & 31) == 0) red[q >> 5] = tot;
+  __syncthreads();
+  if (q == 0) {
+    const long long sum = red[0] + red[1] + red[2] + red[3];
     P.act[t] = 0;
-    if (tot) atomicAdd(P.flow + inst, (unsigned long long)tot);
+    if (sum) atomicAdd(P.flow + inst, (unsigned long long)sum);
   }
 }
 
-// Both cut sets of every instance into its bound device outputs (1/0 bytes).
-__global__ void __launch_bounds__(512) k_seg_all(DevPool P, uint8_t* const* __restrict__ out) {
+// Both cut sets of every instance into its bound device outputs (1/0 bytes):
+// a CTA of 128 threads per tile, four voxels of a row per thread.  The
+// height and source-set loads depend only on the tile and go first.
+__global__ void __launch_bounds__(128) k_seg_all(DevPool P, uint8_t* const* __restrict__ out) {
   const int t = blockIdx.x;
+  const int l0 = 4 * threadIdx.x;
+  const int64_t g0 = (int64_t)t * TV + l0;
+  const int4 h = __ldcg(reinterpret_cast<const int4*>(P.h + g0));
+  const unsigned rc = __ldcg(reinterpret_cast<const unsigned int*>(P.reach + g0));
   const int inst = P.tinst[t];
   const InstGeo G = P.geo[inst];
-  const int lt = t - G.tile_base;
-  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
-  const int l = threadIdx.x;
-  const int x = tx * 8 + (l & 7), y = ty * 8 + ((l >> 3) & 7), z = tz * 8 + (l >> 6);
-  if (x >= G.X || y >= G.Y || z >= G.Z) return;
-  const int64_t g = (int64_t)t * TV + l;
-  const int64_t v = x + (int64_t)G.X * (y + (int64_t)G.Y * z);
   uint8_t* src = out[2 * inst];
   uint8_t* snk = out[2 * inst + 1];
-  if (src) src[v] = P.reach[g] ? 1 : 0;
-  if (snk) snk[v] = P.h[g] < INF ? 1 : 0;
+  const int lt = t - G.tile_base;
+  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
+  const int x0 = tx * 8 + (l0 & 7), y = ty * 8 + ((l0 >> 3) & 7), z = tz * 8 + (l0 >> 6);
+  if (x0 >= G.X || y >= G.Y || z >= G.Z) return;
+  const int hv[4] = {h.x, h.y, h.z, h.w};
+  const int64_t v0 = x0 + (int64_t)G.X * (y + (int64_t)G.Y * z);
+  const int n = min(4, G.X - x0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k >= n) break;
+    if (src) src[v0 + k] = ((rc >> (8 * k)) & 0xffu) ? 1 : 0;
+    if (snk) snk[v0 + k] = hv[k] < INF ? 1 : 0;
+  }
 }
 
 static int ensure_tables(Pool& p) {
@@ -161,7 +223,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, stream));
-  k_put_all<<<d.T, 512, 0, stream>>>(d, p.d_in);
+  k_put_all<<<d.T, 128, 0, stream>>>(d, p.d_in);
   note_launch();
   SolveParams prm;
   prm.L = o.local_pulses;
@@ -178,7 +240,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   bool any_out = false;
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;
   if (any_out) {
-    k_seg_all<<<d.T, 512, 0, stream>>>(d, p.d_out);
+    k_seg_all<<<d.T, 128, 0, stream>>>(d, p.d_out);
     note_launch();
   }
   if (flows_dev) CGC_CUDA(cudaMemcpyAsync(flows_dev, d.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToDevice, stream));
