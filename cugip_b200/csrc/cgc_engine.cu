@@ -96,7 +96,11 @@ __global__ void __launch_bounds__(512) k_put_nlinks(DevPool P, int inst, int axi
 // graph_cut_push.hpp:11-24): the t-links of a voxel cancel,
 // m = min(capS, capT) goes straight from the source to the sink, the rest of
 // capS becomes excess.  Also checks that no excess or residual can exceed
-// int32 and builds the residual bit mask.
+// int32 and builds the residual bit mask.  The kernel is bound by load
+// latency: the face neighbours are read first (the same six values for the
+// whole tile), then all fourteen per-voxel loads are issued at once, with the
+// index of a missing neighbour clamped to the voxel itself and the value
+// masked afterwards.
 __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   __shared__ long long red[16];
   const int t = blockIdx.x;
@@ -104,7 +108,20 @@ __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
   const int64_t Np = P.Np;
+  int nbt[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) nbt[d] = __ldg(P.nbr + d * P.T + t);
   const int s = P.e[g], c = P.rT[g];
+  int rv[6], bk[6];
+  bool has[6];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    const bool in = inside(d, x, y, z);
+    has[d] = in || nbt[d] >= 0;
+    const int64_t ng = in ? g + loff(d) : (has[d] ? (int64_t)nbt[d] * TV + l + xoff(d) : g);
+    rv[d] = P.r[d * Np + g];
+    bk[d] = P.r[(d ^ 1) * Np + ng];
+  }
   const int mcap = min(s, c);
   const int e = s - mcap, rT = c - mcap;
   long long inflow = e;
@@ -112,20 +129,11 @@ __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   bool bad = false;
 #pragma unroll
   for (int d = 0; d < 6; ++d) {
-    const int rv = P.r[d * Np + g];
-    int64_t ng;
-    bool has = true;
-    if (inside(d, x, y, z)) ng = (int64_t)t * TV + l + loff(d);
-    else {
-      const int nt = P.nbr[d * P.T + t];
-      has = nt >= 0;
-      ng = (int64_t)nt * TV + l + xoff(d);
-    }
-    const long long back = has ? (long long)P.r[(d ^ 1) * Np + ng] : 0ll;
-    if (!has && rv != 0) bad = true;  // capacity towards the outside of the grid
+    const long long back = has[d] ? (long long)bk[d] : 0ll;
+    if (!has[d] && rv[d] != 0) bad = true;  // capacity towards the outside of the grid
     inflow += back;
-    if ((long long)rv + back > 2147483647ll) bad = true;
-    m |= (rv > 0 ? 1u : 0u) << d;
+    if ((long long)rv[d] + back > 2147483647ll) bad = true;
+    m |= (rv[d] > 0 ? 1u : 0u) << d;
   }
   if (inflow > 2147483647ll) bad = true;
   if (bad) raise_error(P, CGC_ERR_OVERFLOW);
@@ -744,6 +752,35 @@ __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t
   }
 }
 
+// The same per tile of instance inst: a CTA of 128 threads per tile, four
+// voxels of a row per thread (one 16-byte or 4-byte load), no division per
+// voxel.
+__global__ void __launch_bounds__(128) k_segments_tiles(DevPool P, int inst, int which, uint8_t* out, uint8_t mask,
+                                                        uint8_t bg) {
+  const InstGeo G = P.geo[inst];
+  const int lt = blockIdx.x;
+  const int t = G.tile_base + lt;
+  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
+  const int l0 = 4 * threadIdx.x;
+  const int x0 = tx * 8 + (l0 & 7), y = ty * 8 + ((l0 >> 3) & 7), z = tz * 8 + (l0 >> 6);
+  if (x0 >= G.X || y >= G.Y || z >= G.Z) return;
+  const int64_t g0 = (int64_t)t * TV + l0;
+  bool in[4];
+  if (which == CGC_SEG_SINK_REACH) {
+    const int4 h = __ldcg(reinterpret_cast<const int4*>(P.h + g0));
+    in[0] = h.x < INF; in[1] = h.y < INF; in[2] = h.z < INF; in[3] = h.w < INF;
+  } else {
+    const unsigned rc = __ldcg(reinterpret_cast<const unsigned int*>(P.reach + g0));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) in[k] = ((rc >> (8 * k)) & 0xffu) != 0;
+  }
+  const int64_t v0 = x0 + (int64_t)G.X * (y + (int64_t)G.Y * z);
+  const int n = min(4, G.X - x0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < n) out[v0 + k] = in[k] ? mask : bg;
+}
+
 __global__ void k_unpermute(DevPool P, int inst, const int32_t* plane, int32_t* out) {
   const InstGeo G = P.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
@@ -1167,8 +1204,8 @@ int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
   uint8_t* dst = host ? p.seg : out;
-  const int blocks = (int)std::min<int64_t>((N + 255) / 256, 65535);
-  k_segments<<<blocks, 256, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
+  const int tiles = G.TX * G.TY * G.TZ;
+  k_segments_tiles<<<tiles, 128, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
   CGC_CUDA(cudaGetLastError());
   if (host) CGC_CUDA(cudaMemcpyAsync(out, p.seg, N, cudaMemcpyDeviceToHost, p.stream));
   CGC_CUDA(cudaStreamSynchronize(p.stream));
