@@ -141,31 +141,22 @@ __global__ void __launch_bounds__(128) k_put_all(DevPool P, const int32_t* const
   }
 }
 
-// Both cut sets of every instance into its bound device outputs (1/0 bytes):
-// a CTA of 128 threads per tile, four voxels of a row per thread.  The
-// height and source-set loads depend only on the tile and go first.
-__global__ void __launch_bounds__(128) k_seg_all(DevPool P, uint8_t* const* __restrict__ out) {
-  const int t = blockIdx.x;
-  const int l0 = 4 * threadIdx.x;
-  const int64_t g0 = (int64_t)t * TV + l0;
-  const int4 h = __ldcg(reinterpret_cast<const int4*>(P.h + g0));
-  const unsigned rc = __ldcg(reinterpret_cast<const unsigned int*>(P.reach + g0));
-  const int inst = P.tinst[t];
+// Both cut sets of every instance into its bound device outputs (1/0 bytes),
+// in linear voxel order: grid row blockIdx.y is the instance, its CTAs stride
+// over it four voxels per thread (seg_gather4 / seg_store4).
+__global__ void __launch_bounds__(256) k_seg_all(DevPool P, uint8_t* const* __restrict__ out) {
+  const int inst = blockIdx.y;
   const InstGeo G = P.geo[inst];
   uint8_t* src = out[2 * inst];
   uint8_t* snk = out[2 * inst + 1];
-  const int lt = t - G.tile_base;
-  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
-  const int x0 = tx * 8 + (l0 & 7), y = ty * 8 + ((l0 >> 3) & 7), z = tz * 8 + (l0 >> 6);
-  if (x0 >= G.X || y >= G.Y || z >= G.Z) return;
-  const int hv[4] = {h.x, h.y, h.z, h.w};
-  const int64_t v0 = x0 + (int64_t)G.X * (y + (int64_t)G.Y * z);
-  const int n = min(4, G.X - x0);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    if (k >= n) break;
-    if (src) src[v0 + k] = ((rc >> (8 * k)) & 0xffu) ? 1 : 0;
-    if (snk) snk[v0 + k] = hv[k] < INF ? 1 : 0;
+  if (!src && !snk) return;
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  for (int64_t v0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); v0 < N;
+       v0 += 4 * (int64_t)gridDim.x * blockDim.x) {
+    unsigned a = 0, b = 0;
+    seg_gather4(P, G, v0, N, snk ? &a : nullptr, src ? &b : nullptr);
+    if (src) seg_store4(src, v0, N, b, 1, 0);
+    if (snk) seg_store4(snk, v0, N, a, 1, 0);
   }
 }
 
@@ -240,7 +231,8 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   bool any_out = false;
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;
   if (any_out) {
-    k_seg_all<<<d.T, 128, 0, stream>>>(d, p.d_out);
+    const unsigned gx = (unsigned)std::min<int64_t>(std::max<int64_t>((p.maxN + 32767) / 32768, 1), 4096);
+    k_seg_all<<<dim3(gx, (unsigned)p.ninst), 256, 0, stream>>>(d, p.d_out);
     note_launch();
   }
   if (flows_dev) CGC_CUDA(cudaMemcpyAsync(flows_dev, d.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToDevice, stream));

@@ -752,33 +752,19 @@ __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t
   }
 }
 
-// The same per tile of instance inst: a CTA of 128 threads per tile, four
-// voxels of a row per thread (one 16-byte or 4-byte load), no division per
-// voxel.
-__global__ void __launch_bounds__(128) k_segments_tiles(DevPool P, int inst, int which, uint8_t* out, uint8_t mask,
-                                                        uint8_t bg) {
+// The same in linear voxel order, four voxels per thread (seg_gather4 /
+// seg_store4).
+__global__ void __launch_bounds__(256) k_segments_lin(DevPool P, int inst, int which, uint8_t* out, uint8_t mask,
+                                                      uint8_t bg) {
   const InstGeo G = P.geo[inst];
-  const int lt = blockIdx.x;
-  const int t = G.tile_base + lt;
-  const int tx = lt % G.TX, ty = (lt / G.TX) % G.TY, tz = lt / (G.TX * G.TY);
-  const int l0 = 4 * threadIdx.x;
-  const int x0 = tx * 8 + (l0 & 7), y = ty * 8 + ((l0 >> 3) & 7), z = tz * 8 + (l0 >> 6);
-  if (x0 >= G.X || y >= G.Y || z >= G.Z) return;
-  const int64_t g0 = (int64_t)t * TV + l0;
-  bool in[4];
-  if (which == CGC_SEG_SINK_REACH) {
-    const int4 h = __ldcg(reinterpret_cast<const int4*>(P.h + g0));
-    in[0] = h.x < INF; in[1] = h.y < INF; in[2] = h.z < INF; in[3] = h.w < INF;
-  } else {
-    const unsigned rc = __ldcg(reinterpret_cast<const unsigned int*>(P.reach + g0));
-#pragma unroll
-    for (int k = 0; k < 4; ++k) in[k] = ((rc >> (8 * k)) & 0xffu) != 0;
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  for (int64_t v0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); v0 < N;
+       v0 += 4 * (int64_t)gridDim.x * blockDim.x) {
+    unsigned bits = 0;
+    if (which == CGC_SEG_SINK_REACH) seg_gather4(P, G, v0, N, &bits, nullptr);
+    else seg_gather4(P, G, v0, N, nullptr, &bits);
+    seg_store4(out, v0, N, bits, mask, bg);
   }
-  const int64_t v0 = x0 + (int64_t)G.X * (y + (int64_t)G.Y * z);
-  const int n = min(4, G.X - x0);
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-    if (k < n) out[v0 + k] = in[k] ? mask : bg;
 }
 
 __global__ void k_unpermute(DevPool P, int inst, const int32_t* plane, int32_t* out) {
@@ -1204,8 +1190,8 @@ int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
   uint8_t* dst = host ? p.seg : out;
-  const int tiles = G.TX * G.TY * G.TZ;
-  k_segments_tiles<<<tiles, 128, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
+  const unsigned blocks = (unsigned)std::min<int64_t>(std::max<int64_t>((N + 1023) / 1024, 1), 8 * (int64_t)p.sms);
+  k_segments_lin<<<blocks, 256, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
   CGC_CUDA(cudaGetLastError());
   if (host) CGC_CUDA(cudaMemcpyAsync(out, p.seg, N, cudaMemcpyDeviceToHost, p.stream));
   CGC_CUDA(cudaStreamSynchronize(p.stream));

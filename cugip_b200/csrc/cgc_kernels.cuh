@@ -354,6 +354,58 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 }
 
 // ---------------------------------------------------------------------------
+// Cut sets in linear voxel order, four voxels per thread: voxels v0..v0+3 of
+// an instance (v0 a multiple of 4) are gathered from the tile layout (one
+// 64-bit division per four voxels, all loads issued at once from clamped
+// indices), and the four output bytes go out as one 32-bit store when the
+// destination is aligned, so a warp writes whole 128-byte lines.
+// Bit 0 of each byte of *sink: height < INF; of *source: in the minimal
+// source set.
+__device__ __forceinline__ void seg_gather4(const DevPool& P, const InstGeo& G, int64_t v0, int64_t N,
+                                            unsigned* sink, unsigned* source) {
+  int64_t rest = v0 / G.X;
+  int x = (int)(v0 - rest * G.X);
+  int y = (int)(rest % G.Y), z = (int)(rest / G.Y);
+  int64_t gk[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int64_t t = G.tile_base + (x >> 3) + (int64_t)G.TX * ((y >> 3) + (int64_t)G.TY * (z >> 3));
+    gk[k] = t * TV + (x & 7) + 8 * (y & 7) + 64 * (z & 7);
+    if (v0 + k >= N) gk[k] = gk[0];
+    if (++x == G.X) { x = 0; if (++y == G.Y) { y = 0; ++z; } }
+  }
+  unsigned a = 0, b = 0;
+  int hv[4];
+  unsigned char rv[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    hv[k] = sink ? __ldcg(P.h + gk[k]) : INF;
+    rv[k] = source ? __ldcg(P.reach + gk[k]) : (unsigned char)0;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    a |= (hv[k] < INF ? 1u : 0u) << (8 * k);
+    b |= (rv[k] ? 1u : 0u) << (8 * k);
+  }
+  if (sink) *sink = a;
+  if (source) *source = b;
+}
+
+// the bytes of `bits` (0 or 1 each) as mask / bg at out[v0 .. min(v0 + 4, N))
+__device__ __forceinline__ void seg_store4(uint8_t* out, int64_t v0, int64_t N, unsigned bits, uint8_t mask,
+                                           uint8_t bg) {
+  unsigned w = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) w |= (unsigned)(((bits >> (8 * k)) & 1u) ? mask : bg) << (8 * k);
+  uint8_t* p = out + v0;
+  if (v0 + 4 <= N && ((reinterpret_cast<uintptr_t>(p) & 3u) == 0)) {
+    *reinterpret_cast<unsigned*>(p) = w;
+  } else {
+    for (int k = 0; k < 4 && v0 + k < N; ++k) p[k] = (uint8_t)(w >> (8 * k));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // BFS seeding, first step: bfs_init_tile_w (a warp per tile).
 // Second BFS seeding step, one thread per tile: queue every tile that is not
 // all seeds and holds a seed or touches a seed on a neighbour's face.
