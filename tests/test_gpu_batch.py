@@ -155,3 +155,45 @@ def test_bound_inputs_are_checked_like_host_uploads():
         assert e.value.code == 6
     finally:
         B.close()
+
+
+@pytest.mark.parametrize("offset", [1, 3])
+def test_outputs_at_unaligned_addresses(device_batch, offset):
+    """Cut sets written to device buffers that start off a 4-byte boundary
+    (byte stores instead of word stores), for instances whose voxel counts
+    are not multiples of 4: the same bytes as the golden sets."""
+    import torch
+    B, vols, ins, outs, flows = device_batch
+    dev = torch.device("cuda", 0)
+    raw = [(torch.full((v.N + 8,), 7, dtype=torch.uint8, device=dev),
+            torch.full((v.N + 8,), 7, dtype=torch.uint8, device=dev)) for v in vols]
+    try:
+        for i, r in enumerate(raw):
+            B.bind_outputs(i, r[0].data_ptr() + offset, r[1].data_ptr() + offset)
+        B.enqueue(Policy(), flows.data_ptr())
+        fl = B.wait()
+        shifted = [(r[0][offset:offset + v.N], r[1][offset:offset + v.N]) for r, v in zip(raw, vols)]
+        _check(shifted, fl)
+        for r, v in zip(raw, vols):  # nothing written around the outputs
+            for buf in r:
+                assert int(buf[:offset].ne(7).sum()) == 0
+                assert int(buf[offset + v.N:].ne(7).sum()) == 0
+    finally:
+        for i, o in enumerate(outs):
+            B.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
+    # the single-grid device output path
+    v, d = vols[0], ins[0]  # 151 x 99 x 147: the voxel count is not a multiple of 4
+    G = GridGraph(v.X, v.Y, v.Z)
+    try:
+        G.set_tweights_device(d[0].data_ptr(), d[1].data_ptr())
+        for ax in range(3):
+            G.set_nweights_device(ax, d[2 + ax].data_ptr())
+        assert G.max_flow() == CASES[KEYS[0]]["flow"]
+        buf = torch.full((v.N + 8,), 7, dtype=torch.uint8, device=dev)
+        G.fill_segments_device(buf.data_ptr() + offset, 1, 0, SOURCE)
+        assert sha(buf[offset:offset + v.N].cpu().numpy()) == CASES[KEYS[0]]["smin_sha256"]
+        assert int(buf[:offset].ne(7).sum()) == 0 and int(buf[offset + v.N:].ne(7).sum()) == 0
+        G.fill_segments_device(buf.data_ptr() + offset, 1, 0, SINK)
+        assert sha(buf[offset:offset + v.N].cpu().numpy()) == CASES[KEYS[0]]["treach_sha256"]
+    finally:
+        G.close()
