@@ -739,7 +739,9 @@ __global__ void __launch_bounds__(WARP_CTA_WARPS * 32, 1) k_solve_w(DevPool P, S
   solve_body<true>(P, prm, wsmem);
 }
 
-// Output kernels (linear layout of one instance).
+// Output kernels (linear layout of one instance).  k_segments, a thread per
+// voxel, serves the allocation-free entry point; grids and batches use
+// k_segments_lin / k_seg_all (four voxels per thread).
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg) {
   const InstGeo G = P.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
