@@ -390,13 +390,23 @@ __device__ inline void reach_init_tile_w(const DevPool& P, const int t, const ui
                                          int32_t* cnt0, const WorkQueue* wq = nullptr) {
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
+  // A seed only spreads along its residual edges: the tile needs a visit if
+  // some seed has one inside the tile (bit 6), and the neighbour across face
+  // f if a seed on that face has one through it (bit f; that neighbour's
+  // visit reads the seed and the edge from its halo).  A seed without
+  // residual edges -- in a maximum flow, typically an isolated excess voxel
+  // whose out-edges are saturated -- is its own closure.
   unsigned flags = 0;
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     const int i = wv_index(lane, k);
-    const bool seed = (__ldcg(P.rmask + base + i) & 128u) != 0;
+    const unsigned m = __ldcg(P.rmask + base + i);
+    const bool seed = (m & 128u) != 0;
     P.reach[base + i] = seed ? 1 : 0;
-    if (seed) flags |= face_bits(wv_x(lane), wv_y(lane, k), wv_z(k)) | 64u;
+    if (seed) {
+      const unsigned fb = (unsigned)face_bits(wv_x(lane), wv_y(lane, k), wv_z(k));
+      flags |= (m & fb & 63u) | ((m & ~fb & 63u) ? 64u : 0u);
+    }
   }
   flags = __reduce_or_sync(FULL, flags);
   if (lane == 0 && (flags & 64u)) enqueue(P, P.stamp_bfs, t, id0, list0, cnt0, wq);
