@@ -142,21 +142,24 @@ __global__ void __launch_bounds__(128) k_put_all(DevPool P, const int32_t* const
 }
 
 // Both cut sets of every instance into its bound device outputs (1/0 bytes),
-// in linear voxel order: grid row blockIdx.y is the instance, its CTAs stride
-// over it four voxels per thread (seg_gather4 / seg_store4).
+// in linear voxel order: grid row blockIdx.y takes instances blockIdx.y,
+// blockIdx.y + gridDim.y, ... (one each unless there are more than 65535),
+// and its CTAs stride over an instance four voxels per thread
+// (seg_gather4 / seg_store4).
 __global__ void __launch_bounds__(256) k_seg_all(DevPool P, uint8_t* const* __restrict__ out) {
-  const int inst = blockIdx.y;
-  const InstGeo G = P.geo[inst];
-  uint8_t* src = out[2 * inst];
-  uint8_t* snk = out[2 * inst + 1];
-  if (!src && !snk) return;
-  const int64_t N = (int64_t)G.X * G.Y * G.Z;
-  for (int64_t v0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); v0 < N;
-       v0 += 4 * (int64_t)gridDim.x * blockDim.x) {
-    unsigned a = 0, b = 0;
-    seg_gather4(P, G, v0, N, snk ? &a : nullptr, src ? &b : nullptr);
-    if (src) seg_store4(src, v0, N, b, 1, 0);
-    if (snk) seg_store4(snk, v0, N, a, 1, 0);
+  for (int inst = blockIdx.y; inst < P.ninst; inst += gridDim.y) {
+    const InstGeo G = P.geo[inst];
+    uint8_t* src = out[2 * inst];
+    uint8_t* snk = out[2 * inst + 1];
+    if (!src && !snk) continue;
+    const int64_t N = (int64_t)G.X * G.Y * G.Z;
+    for (int64_t v0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); v0 < N;
+         v0 += 4 * (int64_t)gridDim.x * blockDim.x) {
+      unsigned a = 0, b = 0;
+      seg_gather4(P, G, v0, N, snk ? &a : nullptr, src ? &b : nullptr);
+      if (src) seg_store4(src, v0, N, b, 1, 0);
+      if (snk) seg_store4(snk, v0, N, a, 1, 0);
+    }
   }
 }
 
@@ -232,7 +235,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;
   if (any_out) {
     const unsigned gx = (unsigned)std::min<int64_t>(std::max<int64_t>((p.maxN + 32767) / 32768, 1), 4096);
-    k_seg_all<<<dim3(gx, (unsigned)p.ninst), 256, 0, stream>>>(d, p.d_out);
+    k_seg_all<<<dim3(gx, (unsigned)std::min(p.ninst, 65535)), 256, 0, stream>>>(d, p.d_out);
     note_launch();
   }
   if (flows_dev) CGC_CUDA(cudaMemcpyAsync(flows_dev, d.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToDevice, stream));
