@@ -112,8 +112,6 @@ struct DevPool {
   uint8_t* tsink;             // cycles*T: 1 if the tile delivered flow to the sink during the cycle
 };
 
-__host__ __device__ inline int dir_axis(int d) { return d >> 1; }
-
 // parameters of the persistent solve kernel
 struct SolveParams {
   int L;                 // pulses per tile visit (per region-relabel round)
