@@ -145,6 +145,14 @@ def generic_layered() -> dict:
     return {"ms": min(runs[1:]), "vertices": n, "edges": int(a.size), "flow": flow}
 
 
+def solve_kernel_name(pol) -> str:
+    """The persistent solve kernel a policy launches (cgc_engine.cu launch_solve)."""
+    c = pol.ctas_per_sm or 2
+    if c == 2:
+        return "k_solve"
+    return f"k_solve{c}" + ("w" if pol.bfs_warp_min else "")
+
+
 def profiled_traffic(workload: int):
     """dram bytes per k_solve launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"k_solve_workload{workload}_traffic.txt")
@@ -434,7 +442,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
-                         "kernel": "k_solve", "kernel_ms": solve_ms, "peak_source": peak_kind,
+                         "kernel": solve_kernel_name(best), "kernel_ms": solve_ms, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes},
             "solver_stats": {k: st[k] for k in ("sweeps", "global_relabels", "bfs_rounds", "tiles_swept",
                                                 "tiles_relabelled", "pulses", "bfs_ms", "sweep_ms", "reach_ms",
@@ -479,8 +487,25 @@ def main():
         tot = sum(x.N for x in vols)
         dins = [[torch.from_numpy(a).to(dev) for a in x.arrays()] for x in vols]
         douts = [torch.zeros((2, x.N), dtype=torch.uint8, device=dev) for x in vols]
+        gold96 = [golden(4, i) for i in range(nb)]
+        have_gold96 = all(c is not None for c in gold96)
+
+        def check_batch(fl, what):
+            """every instance's flow and both bound masks against the oracle's golden answer"""
+            if not have_gold96:
+                if fl != seq_flows:
+                    raise SystemExit(f"{what}: flows differ from the single solves")
+                return
+            for i, c in enumerate(gold96):
+                if fl[i] != c["flow"]:
+                    raise SystemExit(f"{what}: instance {i} flow {fl[i]} differs from the oracle's {c['flow']}")
+                if (sha(douts[i][0].cpu().numpy()) != c["smin_sha256"]
+                        or sha(douts[i][1].cpu().numpy()) != c["treach_sha256"]):
+                    raise SystemExit(f"{what}: instance {i} cut sets differ from the oracle's")
+
         # plain: one solve per instance through the single-grid API
         seq = []
+        seq_kernel_ms = []
         grids = [GridGraph(x.X, x.Y, x.Z) for x in vols]
         for rep in range(2):
             torch.cuda.synchronize()
@@ -496,7 +521,9 @@ def main():
             e1_.record()
             torch.cuda.synchronize()
             seq.append(e0_.elapsed_time(e1_))
+            seq_kernel_ms.append(sum(gg.stats()["kernel_ms"] for gg in grids))
         seq_flows = [gg.flow for gg in grids]
+        check_batch(seq_flows, "plain sequential solves")
         for gg in grids:
             gg.close()
         seq_ms = min(seq)
@@ -513,6 +540,8 @@ def main():
             BB.graph_create(pol)
             ts = []
             for _ in range(reps):
+                for o in douts:
+                    o.fill_(7)
                 torch.cuda.synchronize()
                 e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0_.record()
@@ -520,12 +549,13 @@ def main():
                 e1_.record()
                 fl = BB.wait()
                 ts.append(e0_.elapsed_time(e1_))
-                if fl != seq_flows:
-                    raise SystemExit("batched flows differ from the single solves")
+                check_batch(fl, f"batch {pol!r}")
             return statistics.median(ts)
 
         bat_ms = time_batch(bbest)
-        var["batch96_plain_sequential"] = {"ms": seq_ms, "voxels_per_s": tot / seq_ms * 1e3, "schedule": repr(Policy())}
+        var["batch96_plain_sequential"] = {"ms": seq_ms, "voxels_per_s": tot / seq_ms * 1e3, "schedule": repr(Policy()),
+                                           "sum_of_kernel_ms": min(seq_kernel_ms)}
+        var["batch96_parity"] = "oracle" if have_gold96 else "single solves"
         var["batch96_batched_graph"] = {"ms": bat_ms, "voxels_per_s": tot / bat_ms * 1e3, "schedule": repr(bbest)}
         if have_learned:
             lb = Policy.from_options(bbest.options())

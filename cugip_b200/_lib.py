@@ -19,8 +19,6 @@ ERRORS = {
 }
 SEG_SINK_REACH = 0
 SEG_SOURCE_MIN = 1
-SCHED_PARITY = 0
-SCHED_ASYNC = 1
 
 
 class CgcError(RuntimeError):
@@ -34,10 +32,10 @@ class CgcError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("struct_size", C.c_int32), ("local_pulses", C.c_int32), ("sweeps_per_relabel", C.c_int32),
-                ("schedule", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
+                ("wait_limit_us", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
                 ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("learned", C.c_int32), ("trace_cycles", C.c_int32),
-                ("warp_tiles", C.c_int32), ("bfs_warp_min", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("bfs_warp_min", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class Stats(C.Structure):
@@ -154,21 +152,16 @@ def check(rc: int) -> None:
         raise CgcError(rc, load().cgc_last_error().decode(errors="replace"))
 
 
-def options(local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0, max_sweeps: int = 0,
-            persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0, ctas_per_sm: int = 0,
-            learned: int = 0, trace_cycles: int = 0, warp_tiles: int = 0, bfs_warp_min: int = 0) -> Options:
+OPTION_FIELDS = ("local_pulses", "sweeps_per_relabel", "wait_limit_us", "max_sweeps", "persistent",
+                 "region_relabels", "stall_sweeps", "ctas_per_sm", "learned", "trace_cycles", "bfs_warp_min")
+
+
+def options(**fields) -> Options:
+    """A cgc_options with struct_size set; fields left out are 0 (the default)."""
     o = Options()
     o.struct_size = C.sizeof(Options)
-    o.local_pulses = local_pulses
-    o.sweeps_per_relabel = sweeps_per_relabel
-    o.schedule = schedule
-    o.max_sweeps = max_sweeps
-    o.persistent = persistent
-    o.region_relabels = region_relabels
-    o.stall_sweeps = stall_sweeps
-    o.ctas_per_sm = ctas_per_sm
-    o.learned = learned
-    o.trace_cycles = trace_cycles
-    o.warp_tiles = warp_tiles
-    o.bfs_warp_min = bfs_warp_min
+    for k, v in fields.items():
+        if k not in OPTION_FIELDS:
+            raise TypeError(f"unknown option {k!r}")
+        setattr(o, k, int(v))
     return o

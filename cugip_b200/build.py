@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libcgc.so")
 
 SOURCES = ["cgc_engine.cu", "cgc_batch.cu", "cgc_autotune.cu", "cgc_sched_train.cu", "cgc_noalloc.cu",
            "cgc_build.cu", "cgc_csr.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
-HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h", "cgc_sched.cuh", "cgc_queue.cuh",
+HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h", "cgc_sched.cuh",
            "cgc_sync.cuh", "cgc_warp.cuh"]
 
 NVCC_FLAGS = [

@@ -46,16 +46,16 @@ void load_cache_locked() {
   if (!path) return;
   FILE* f = std::fopen(path, "r");
   if (!f) return;
-  // line: size class (2), L R K ctas stall warp bfs_warp_min, milliseconds
+  // line: size class (2), L R K ctas stall learned bfs_warp_min, milliseconds
   char line[256];
   while (std::fgets(line, sizeof line, f)) {
-    int ib, vb, L, R, K, cta, st, warp, bw;
+    int ib, vb, L, R, K, cta, st, lr, bw;
     double ms;
-    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &warp, &bw, &ms) != 10) continue;
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &lr, &bw, &ms) != 10) continue;
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
     o.local_pulses = L; o.region_relabels = R; o.sweeps_per_relabel = K; o.ctas_per_sm = cta; o.stall_sweeps = st;
-    o.warp_tiles = warp;
+    o.learned = lr;
     o.bfs_warp_min = bw;
     g_cache[{ib, vb}] = {o, ms};
   }
@@ -69,7 +69,7 @@ void store(std::pair<int, int> key, const cgc_options& o, double ms) {
   if (const char* path = std::getenv("CGC_AUTOTUNE_CACHE")) {
     if (FILE* f = std::fopen(path, "a")) {
       std::fprintf(f, "%d %d %d %d %d %d %d %d %d %.6f\n", key.first, key.second, o.local_pulses, o.region_relabels,
-                   o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.warp_tiles, o.bfs_warp_min, ms);
+                   o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.learned, o.bfs_warp_min, ms);
       std::fclose(f);
     }
   }
@@ -77,8 +77,6 @@ void store(std::pair<int, int> key, const cgc_options& o, double ms) {
 
 std::vector<cgc_options> default_candidates() {
   std::vector<cgc_options> c;
-  // the warp-per-tile kernel is left out: it was 2-4x slower on every
-  // measured workload (pass it as an explicit candidate to time it)
   for (int cta : {2, 3, 4})
     for (int R : {1, 2, 4})
       for (int L : {2, 4, 8})

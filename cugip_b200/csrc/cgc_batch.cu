@@ -219,17 +219,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, stream));
   k_put_all<<<d.T, 128, 0, stream>>>(d, p.d_in);
   note_launch();
-  SolveParams prm;
-  prm.L = o.local_pulses;
-  prm.R = o.region_relabels;
-  prm.K = o.sweeps_per_relabel;
-  prm.stall = o.stall_sweeps;
-  prm.learned = o.learned;
-  prm.trace_cycles = o.trace_cycles;
-  prm.max_sweeps = (int64_t)o.max_sweeps;
-  prm.limit_ns = 20ull * 1000000000ull;
-  prm.async = o.schedule == CGC_SCHED_ASYNC ? 1 : 0;
-  prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
+  const SolveParams prm = solve_params(o);
   if (int rc = launch_solve(p, o, d, prm, stream)) return rc;
   bool any_out = false;
   for (uint8_t* q : p.out_ptrs) any_out = any_out || q;

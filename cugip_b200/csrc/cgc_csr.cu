@@ -544,7 +544,7 @@ int graph_maxflow(cgc_graph* g, const cgc_options* opts, int64_t* flow) {
   CsrParams prm;
   prm.K = std::max(1, 2 * o.sweeps_per_relabel);
   prm.max_pulses = (int64_t)o.max_sweeps;
-  prm.limit_ns = 20ull * 1000000000ull;
+  prm.limit_ns = wait_limit_ns(o);
   const long long launches0 = g_launches.load();
   CsrDev& d = g->d;
   cudaEvent_t ev[4] = {};

@@ -84,12 +84,6 @@ struct DevPool {
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
   uint32_t* stamp_sw;   // T: last sweep the tile was queued for
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
-  // work-queue schedule (null if unused): two queues (rings of qcap slots and
-  // their control blocks) and a lock word per tile (LOCK_W | readers)
-  int32_t* qring;       // 2*qcap
-  int32_t* qctl;        // 2*QCTL_INTS
-  int32_t qcap;
-  int32_t* tlock;       // T
   int32_t* cnt;         // C_NCOUNTERS
   unsigned long long* flow;   // ninst: flow value (int64 as two's complement)
   const InstGeo* geo;   // ninst
@@ -122,7 +116,6 @@ struct SolveParams {
   int trace_cycles;      // record scheduling traces for the first trace_cycles relabel cycles
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
-  int async = 0;         // 1: work-queue schedule (CGC_SCHED_ASYNC)
   int bfs_warp_min = 0;  // BFS rounds with at least this many tiles per CTA run a warp per tile (0: never)
 };
 
@@ -136,10 +129,6 @@ __global__ void k_solve3(DevPool P, SolveParams prm);
 __global__ void k_solve4(DevPool P, SolveParams prm);
 __global__ void k_solve3w(DevPool P, SolveParams prm);
 __global__ void k_solve4w(DevPool P, SolveParams prm);
-__global__ void k_solve_q(DevPool P, SolveParams prm);
-__global__ void k_solve_q3(DevPool P, SolveParams prm);
-constexpr int WARP_CTA_WARPS = 10;  // warps of the warp-per-tile solve CTA (one CTA per SM)
-__global__ void k_solve_w(DevPool P, SolveParams prm);
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);
 
 }  // namespace cgc

@@ -274,44 +274,34 @@ union SolveShared {
   SchedShared sched;
 };
 
-// The whole solve in one cooperative launch.  WARP = false: a CTA of 512
-// threads is the unit that visits a tile (SolveShared); WARP = true: every
-// warp of the CTA visits tiles on its own (WarpSmem per warp).
-template <bool WARP, bool BFSW = false>
-__device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, void* smem) {
+// The whole solve in one cooperative launch; a CTA of 512 threads is the unit
+// that visits a tile.
+template <bool BFSW = false>
+__device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& prm, SolveShared& S) {
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
-  SolveShared& S = *reinterpret_cast<SolveShared*>(smem);
-  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem)[WARP ? (tid >> 5) : 0];
-  // tile-visiting units: CTAs or warps
-  const int U = WARP ? G * (int)(blockDim.x >> 5) : G;
-  const int u = WARP ? b * (int)(blockDim.x >> 5) + (tid >> 5) : b;
-  const bool leader = WARP ? (tid & 31) == 0 : tid == 0;
+  const bool leader = tid == 0;
   // warps of the grid, for the passes that visit every tile with a warp
   const int gw = b * (int)(blockDim.x >> 5) + (tid >> 5), nw = G * (int)(blockDim.x >> 5);
-  // Hands out the n entries of a round.  CTA shape: the first entry of CTA b
-  // is entry b; later ones come from the round's counter (C_TAKE0 + round % 3,
-  // the next round's slot is cleared meanwhile) through an atomic issued when
-  // the current visit starts and read when it ends, so visits of uneven cost
-  // spread over the CTAs.  Warp shape: static striding.
+  // Hands out the n entries of a round.  The first entry of CTA b is entry b;
+  // later ones come from the round's counter (C_TAKE0 + round % 3, the next
+  // round's slot is cleared meanwhile) through an atomic issued when the
+  // current visit starts and read when it ends, so visits of uneven cost
+  // spread over the CTAs.
   __shared__ int s_next;
   int round_no = 0;
   auto for_entries = [&](int n, auto&& visit) {
-    if constexpr (WARP) {
-      for (int i = u; i < n; i += U) visit(i);
-    } else {
-      int32_t* take = P.cnt + C_TAKE0 + round_no % 3;
-      if (b == 0 && tid == 0) P.cnt[C_TAKE0 + (round_no + 1) % 3] = 0;
-      ++round_no;
-      int i = b;
-      while (i < n) {
-        int nx = 0;
-        if (tid == 0) nx = atomicAdd(take, 1);
-        visit(i);
-        if (tid == 0) s_next = G + nx;
-        __syncthreads();
-        i = s_next;
-        __syncthreads();
-      }
+    int32_t* take = P.cnt + C_TAKE0 + round_no % 3;
+    if (b == 0 && tid == 0) P.cnt[C_TAKE0 + (round_no + 1) % 3] = 0;
+    ++round_no;
+    int i = b;
+    while (i < n) {
+      int nx = 0;
+      if (tid == 0) nx = atomicAdd(take, 1);
+      visit(i);
+      if (tid == 0) s_next = G + nx;
+      __syncthreads();
+      i = s_next;
+      __syncthreads();
     }
   };
   int32_t* const bl[3] = {P.lists, P.lists + P.T, P.lists + 2 * P.T};
@@ -359,7 +349,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const int n = ld_cnt(bc + k % 3);
       if (n == 0) break;
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-      if (BFSW && !WARP && n / G >= prm.bfs_warp_min) {
+      if (BFSW && n / G >= prm.bfs_warp_min) {
         // Throughput-bound round: a warp per tile (no block barriers, a
         // tile's relaxation costs one warp's issue slots instead of 16),
         // entries handed out like for_entries, per warp.
@@ -378,8 +368,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
         }
       } else {
         for_entries(n, [&](int i) {
-          if constexpr (WARP) bfs_tile_w(P, __ldcg(bl[k % 3] + i), W.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-          else bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+          bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
         });
       }
       ++k;
@@ -445,12 +434,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
           return;
         }
         const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
-        if constexpr (WARP)
-          sweep_tile_w<true>(P, t, L, prm.R, W.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                             (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
-        else
-          sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                           (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
+        sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
+                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
       });
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
@@ -480,8 +465,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     if (n == 0) break;
     if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
     for_entries(n, [&](int i) {
-      if constexpr (WARP) reach_tile_w(P, __ldcg(bl[k % 3] + i), W.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
-      else reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+      reach_tile(P, __ldcg(bl[k % 3] + i), S.rc, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
     });
     ++k;
     if (!grid_sync(P, prm.limit_ns)) return;
@@ -501,173 +485,6 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   }
 }
 
-// The solve kernel at 2 CTAs per SM (64 registers) and at 3 (40 registers,
-// a few spills).
-// ---------------------------------------------------------------------------
-// The whole solve in one cooperative launch under the work-queue schedule
-// (CGC_SCHED_ASYNC).  A relabel cycle is: exact global relabel (BFS seeded
-// from the sink links, drained through the work queue), then push-relabel
-// visits of the active tiles through the work queue, with tile locks, until
-// the queue is empty or K visits per initially active tile were made.  The
-// phases of a cycle are separated by grid barriers; inside a phase no CTA
-// waits for another.  The end state is the one of the parity schedule: after
-// an exact relabel no tile holds an active vertex, so the preflow is maximum,
-// and the cut sets are computed from the final residual graph.
-__device__ __forceinline__ void solve_async(const DevPool& P, const SolveParams& prm, SolveShared& S) {
-  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
-  const int gtid = b * blockDim.x + tid, nthr = G * blockDim.x;
-  const int gw = b * (int)(blockDim.x >> 5) + (tid >> 5), nw = G * (int)(blockDim.x >> 5);
-  __shared__ int s_take;
-  // queue A: BFS and reachability; queue B: push-relabel visits
-  const WorkQueue qa{P.qring, P.qcap, P.qctl, prm.limit_ns};
-  const WorkQueue qb{P.qring + P.qcap, P.qcap, P.qctl + QCTL_INTS, prm.limit_ns};
-  uint32_t bfs_id = 1, sw_id = 1;
-  long long relabels = 0, cycles = 0;
-  unsigned long long ns_bfs = 0, ns_sweep = 0, ns_reach = 0, ns_sched = 0;
-  int traced = 0;
-  uint64_t tmark = globaltimer_ns();
-  const uint64_t t_launch = tmark;
-  int ntrace = 0;
-  auto record = [&](unsigned long long kind, long long index, int tiles) {
-    if (b == 0 && tid == 0 && P.trace && ntrace < TRACE_CAP) {
-      P.trace[2 * ntrace] = (kind << 56) | ((unsigned long long)(index & 0xffffffffll) << 24) | (unsigned)(tiles & 0xffffff);
-      P.trace[2 * ntrace + 1] = globaltimer_ns() - t_launch;
-      ++ntrace;
-    }
-  };
-  auto lap = [&](unsigned long long& acc) {
-    const uint64_t now = globaltimer_ns();
-    acc += now - tmark;
-    tmark = now;
-  };
-  // both queues empty, no locks held (all CTAs, then a barrier)
-  auto reset_queues = [&]() {
-    for (int i = gtid; i < 2 * P.qcap; i += nthr) P.qring[i] = -1;
-    for (int i = gtid; i < P.T; i += nthr) P.tlock[i] = 0;
-    for (int i = gtid; i < 2 * QCTL_INTS; i += nthr) P.qctl[i] = 0;
-  };
-  // Visits tiles from queue q until the phase is over: q is drained (kind 0:
-  // BFS, 2: reachability) or, for push-relabel visits (kind 1), also once
-  // `budget` visits were made.
-  SweepExtra ex;
-  bool learned = false;
-  auto drain = [&](const WorkQueue& q, int kind, uint32_t id, int budget) {
-    if (ld_volatile(q.c(Q_PENDING)) == 0) return;  // nothing was queued
-    for (;;) {
-      if (tid == 0) {
-        int t = -1;  // -1: leave
-        const uint64_t t0 = globaltimer_ns();
-        for (;;) {
-          const int got = wq_take(q, P.err);
-          if (got == -2) raise_error(P, CGC_ERR_TIMEOUT);
-          if (got < 0) break;
-          if (kind != 1 || tile_try_lock(P, got)) {
-            atomicExch((kind == 1 ? P.stamp_sw : P.stamp_bfs) + got, 0u);  // may be queued again from now on
-            __threadfence();
-            t = got;
-            break;
-          }
-          // a face neighbour is being visited: back into the queue (its stamp
-          // is still set); this take is released after the new entry exists
-          if (!wq_push(q, got)) { raise_error(P, CGC_ERR_TIMEOUT); break; }
-          wq_release(q);
-          if (globaltimer_ns() - t0 > prm.limit_ns) { raise_error(P, CGC_ERR_TIMEOUT); break; }
-          __nanosleep(256);
-        }
-        s_take = t;
-      }
-      __syncthreads();
-      const int t = s_take;
-      __syncthreads();
-      if (t < 0) break;
-      if (kind == 0) {
-        bfs_tile(P, t, S.bfs, id, nullptr, nullptr, &q);
-      } else if (kind == 2) {
-        reach_tile(P, t, S.rc, id, nullptr, nullptr, &q);
-      } else {
-        const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
-        sweep_tile<true>(P, t, L, prm.R, S.sw, id, nullptr, nullptr, id, nullptr, nullptr, ex, &q);
-      }
-      if (tid == 0) {
-        if (kind == 1 && atomicAdd(q.c(Q_VISITS), 1) + 1 == budget) atomicExch(q.c(Q_DONE), 1);
-        wq_release(q);
-      }
-    }
-  };
-
-  for (;;) {
-    // ------------------------------------------------ exact global relabel
-    reset_queues();
-    if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);
-    if (!grid_sync(P, prm.limit_ns)) return;
-    ++bfs_id;
-    for (int t = gtid; t < P.T; t += nthr)
-      if (bfs_seed_tile(P, t)) enqueue(P, P.stamp_bfs, t, bfs_id, nullptr, nullptr, &qa);
-    if (!grid_sync(P, prm.limit_ns)) return;
-    drain(qa, 0, bfs_id, 0);
-    if (!grid_sync(P, prm.limit_ns)) return;
-    ++relabels;
-    record(TR_BFS_ROUND, relabels, 0);
-    lap(ns_bfs);
-    // ------------------------------------------------ active tiles -> queue B
-    ++sw_id;
-    for (int t = gtid; t < P.T; t += nthr)
-      if (__ldcg(P.act + t)) enqueue(P, P.stamp_sw, t, sw_id, nullptr, nullptr, &qb);
-    if (!grid_sync(P, prm.limit_ns)) return;
-    const int nact = ld_volatile(qb.c(Q_PENDING));
-    record(TR_RELABEL_DONE, relabels, nact);
-    if (nact == 0) break;
-    if ((cycles + 1) * 2 * (long long)prm.K > prm.max_sweeps) {
-      if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
-      break;
-    }
-    // ------------------------------------------------ learned scheduler
-    const int cycle = (int)relabels - 1;
-    const bool tracing = prm.trace_cycles > cycle;
-    if (tracing) traced = cycle + 1;
-    learned = prm.learned && nact > 2 * G;
-    if (learned || tracing) {
-      if (!sched_stage(P, prm, cycle, learned, tracing)) return;
-      lap(ns_sched);
-    }
-    // ------------------------------------------------ push-relabel visits
-    ex = SweepExtra();
-    if (tracing) {
-      ex.tr_pulses = P.tpulses + (int64_t)cycle * P.T;
-      ex.tr_sink = P.tsink + (int64_t)cycle * P.T;
-    }
-    const long long budget = (long long)prm.K * nact;
-    drain(qb, 1, sw_id, (int)(budget < (1ll << 30) ? budget : (1ll << 30)));
-    if (!grid_sync(P, prm.limit_ns)) return;
-    ++cycles;
-    record(TR_SWEEP, cycles, ld_volatile(qb.c(Q_VISITS)));
-    lap(ns_sweep);
-  }
-  lap(ns_bfs);
-  // ------------------------------------------------ source-side reachability
-  reset_queues();
-  if (!grid_sync(P, prm.limit_ns)) return;
-  ++bfs_id;
-  for (int t = gw; t < P.T; t += nw) reach_init_tile_w(P, t, bfs_id, nullptr, nullptr, &qa);
-  if (!grid_sync(P, prm.limit_ns)) return;
-  drain(qa, 2, bfs_id, 0);
-  if (!grid_sync(P, prm.limit_ns)) return;
-  record(TR_REACH_ROUND, 1, 0);
-  if (b == 0 && tid == 0) {
-    P.stats[S_SWEEPS] = (unsigned long long)cycles;
-    P.stats[S_RELABELS] = (unsigned long long)relabels;
-    P.stats[S_ROUNDS] = (unsigned long long)relabels;
-    lap(ns_reach);
-    P.stats[S_NS_BFS] = ns_bfs;
-    P.stats[S_NS_SWEEP] = ns_sweep;
-    P.stats[S_NS_REACH] = ns_reach;
-    P.stats[S_TRACE_N] = (unsigned long long)ntrace;
-    P.stats[S_TRACE_CYC] = (unsigned long long)traced;
-    P.stats[S_NS_SCHED] = ns_sched;
-  }
-}
-
 int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -676,67 +493,41 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cfg.stream = stream;
-  if (o.warp_tiles && !prm.async) {
-    cfg.gridDim = dim3(p.coop_blocks_w);
-    cfg.blockDim = dim3(WARP_CTA_WARPS * 32);
-    cfg.dynamicSmemBytes = kWarpSmemBytes;
-    CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_w, d, prm));
-  } else {
-    const bool three = o.ctas_per_sm == 3, four = o.ctas_per_sm == 4 && !prm.async;
-    cfg.gridDim = dim3(four ? p.coop_blocks4 : three ? p.coop_blocks3 : p.coop_blocks);
-    cfg.blockDim = dim3(512);
-    cfg.dynamicSmemBytes = 0;
-    if (prm.async) {
-      if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q3, d, prm));
-      else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve_q, d, prm));
-    } else {
-      const bool bw = prm.bfs_warp_min > 0;
-      if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve4w : k_solve4, d, prm));
-      else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve3w : k_solve3, d, prm));
-      else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
-    }
-  }
+  const bool three = o.ctas_per_sm == 3, four = o.ctas_per_sm == 4;
+  cfg.gridDim = dim3(four ? p.coop_blocks4 : three ? p.coop_blocks3 : p.coop_blocks);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = 0;
+  const bool bw = prm.bfs_warp_min > 0;
+  if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve4w : k_solve4, d, prm));
+  else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve3w : k_solve3, d, prm));
+  else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
   note_launch();
   return ok();
 }
 
+// The solve kernel at 2 CTAs per SM (64 registers), at 3 (40 registers, a
+// few spills) and at 4 (2048 threads, 32 registers).
 __global__ void __launch_bounds__(512, 2) k_solve(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body<false>(P, prm, &S);
+  solve_body(P, prm, S);
 }
 __global__ void __launch_bounds__(512, 3) k_solve3(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body<false>(P, prm, &S);
+  solve_body(P, prm, S);
 }
-// 4 CTAs per SM (2048 threads, 32 registers)
 __global__ void __launch_bounds__(512, 4) k_solve4(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body<false>(P, prm, &S);
+  solve_body(P, prm, S);
 }
 // The same with warp-per-tile BFS rounds (SolveParams::bfs_warp_min); separate
 // kernels, so that the others do not carry that code's registers.
 __global__ void __launch_bounds__(512, 3) k_solve3w(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body<false, true>(P, prm, &S);
+  solve_body<true>(P, prm, S);
 }
 __global__ void __launch_bounds__(512, 4) k_solve4w(DevPool P, SolveParams prm) {
   __shared__ SolveShared S;
-  solve_body<false, true>(P, prm, &S);
-}
-// The solve under the work-queue schedule, at 2 and 3 CTAs per SM.
-__global__ void __launch_bounds__(512, 2) k_solve_q(DevPool P, SolveParams prm) {
-  __shared__ SolveShared S;
-  solve_async(P, prm, S);
-}
-__global__ void __launch_bounds__(512, 3) k_solve_q3(DevPool P, SolveParams prm) {
-  __shared__ SolveShared S;
-  solve_async(P, prm, S);
-}
-// Warp per tile: one CTA of WARP_CTA_WARPS warps per SM, each warp with its
-// own WarpSmem slice of dynamic shared memory.
-__global__ void __launch_bounds__(WARP_CTA_WARPS * 32, 1) k_solve_w(DevPool P, SolveParams prm) {
-  extern __shared__ __align__(16) unsigned char wsmem[];
-  solve_body<true>(P, prm, wsmem);
+  solve_body<true>(P, prm, S);
 }
 
 // Output kernels (linear layout of one instance).  k_segments, a thread per
@@ -842,10 +633,6 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   const int64_t o_sb = off; off += al(T * 4);
   const int64_t o_ss = off; off += al(T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
-  const int64_t o_lk = off; off += al(T * 4);
-  const int32_t qcap = queue_capacity((int32_t)T);
-  const int64_t o_qr = off; off += al(2 * (int64_t)qcap * 4);
-  const int64_t o_qc = off; off += al(2 * QCTL_INTS * 4);
   const int64_t o_cnt = off; off += al(C_NCOUNTERS * 4);
   const int64_t o_fl = off; off += al((int64_t)count * 8);
   const int64_t o_geo = off; off += al((int64_t)count * sizeof(InstGeo));
@@ -862,8 +649,7 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
   d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
   d.act = (uint8_t*)(base + o_act); d.tflag = (uint16_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
-  d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt); d.tlock = (int32_t*)(base + o_lk);
-  d.qring = (int32_t*)(base + o_qr); d.qctl = (int32_t*)(base + o_qc); d.qcap = qcap;
+  d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
   d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
   d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
   d.trace = (unsigned long long*)(base + o_tr);
@@ -911,16 +697,6 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ4w, k_solve4w, 512, 0));
   p->coop_blocks4 = std::max(1, std::min(occ4, occ4w)) * p->sms;
   p->coop_blocks3 = std::min(p->coop_blocks3, std::max(1, occ3w) * p->sms);
-  // the work-queue kernels have the same launch bounds; take the smaller grid
-  int occq = 0, occq3 = 0;
-  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, k_solve_q, 512, 0));
-  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq3, k_solve_q3, 512, 0));
-  p->coop_blocks = std::min(p->coop_blocks, std::max(1, occq) * p->sms);
-  p->coop_blocks3 = std::min(p->coop_blocks3, std::max(1, occq3) * p->sms);
-  CGC_CUDA(cudaFuncSetAttribute(k_solve_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWarpSmemBytes));
-  int occw = 0;
-  CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occw, k_solve_w, WARP_CTA_WARPS * 32, kWarpSmemBytes));
-  p->coop_blocks_w = std::max(1, occw) * p->sms;
   int occ2 = 0;
   CGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_sweep_list, 512, 0));
   p->sweep_blocks = std::max(1, occ2) * p->sms;
@@ -1013,7 +789,7 @@ cgc_options resolve_options(const cgc_options* o) {
   r.struct_size = sizeof(cgc_options);
   r.local_pulses = 4;
   r.sweeps_per_relabel = 8;
-  r.schedule = CGC_SCHED_PARITY;
+  r.wait_limit_us = 20 * 1000 * 1000;
   r.max_sweeps = 1 << 17;
   r.persistent = 1;
   r.region_relabels = 2;
@@ -1022,18 +798,36 @@ cgc_options resolve_options(const cgc_options* o) {
   if (o) {
     if (o->local_pulses > 0) r.local_pulses = std::min(o->local_pulses, 64);
     if (o->sweeps_per_relabel > 0) r.sweeps_per_relabel = o->sweeps_per_relabel;
-    if (o->schedule) r.schedule = o->schedule;
+    if (o->wait_limit_us > 0) r.wait_limit_us = o->wait_limit_us;
     if (o->max_sweeps > 0) r.max_sweeps = o->max_sweeps;
     if (o->persistent) r.persistent = o->persistent;
     if (o->region_relabels) r.region_relabels = o->region_relabels < 0 ? 0 : std::min(o->region_relabels, 16);
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
     if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
-    r.warp_tiles = o->warp_tiles > 0 ? 1 : 0;
     r.bfs_warp_min = o->bfs_warp_min > 0 ? o->bfs_warp_min : 0;
     r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
   return r;
+}
+
+uint64_t wait_limit_ns(const cgc_options& o) {
+  return (uint64_t)(o.wait_limit_us > 0 ? o.wait_limit_us : 20 * 1000 * 1000) * 1000ull;
+}
+
+// Parameters of the persistent solve kernel from resolved options.
+SolveParams solve_params(const cgc_options& o) {
+  SolveParams prm;
+  prm.L = o.local_pulses;
+  prm.R = o.region_relabels;
+  prm.K = o.sweeps_per_relabel;
+  prm.stall = o.stall_sweeps;
+  prm.learned = o.learned;
+  prm.trace_cycles = o.trace_cycles > 0 ? o.trace_cycles : 0;
+  prm.max_sweeps = (int64_t)o.max_sweeps;
+  prm.limit_ns = wait_limit_ns(o);
+  prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
+  return prm;
 }
 
 // host-driven BFS (or reachability) pass; returns rounds executed
@@ -1096,21 +890,11 @@ int pool_solve(Pool& p, const cgc_options* opts) {
 
   int64_t sweeps = 0, relabels = 0, rounds = 0;
   if (o.persistent > 0) {
-    SolveParams prm;
-    prm.L = o.local_pulses;
-    prm.R = o.region_relabels;
-    prm.K = o.sweeps_per_relabel;
-    prm.stall = o.stall_sweeps;
-    prm.learned = o.learned;
-    prm.trace_cycles = o.trace_cycles > 0 ? o.trace_cycles : 0;
+    const SolveParams prm = solve_params(o);
     if (prm.learned || prm.trace_cycles) {
       rc = ensure_sched(p, prm.learned != 0, prm.trace_cycles);
       if (rc) { destroy_events(); return rc; }
     }
-    prm.max_sweeps = (int64_t)o.max_sweeps;
-    prm.limit_ns = 20ull * 1000000000ull;
-    prm.async = o.schedule == CGC_SCHED_ASYNC ? 1 : 0;
-    prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
     CGC_CUDA(cudaEventRecord(evk0, p.stream));
     rc = launch_solve(p, o, d, prm, p.stream);
     if (rc) { destroy_events(); return rc; }

@@ -33,7 +33,6 @@
 #include <cuda_runtime.h>
 #include "cgc.h"
 #include "cgc_device.cuh"
-#include "cgc_queue.cuh"
 
 namespace cgc {
 
@@ -115,17 +114,6 @@ __device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, in
   if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
 }
 
-// queue_tile into the list of the next round, or into the work queue when one
-// is given (asynchronous schedule)
-__device__ __forceinline__ void enqueue(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
-                                        int32_t* cnt, const WorkQueue* wq) {
-  if (atomicExch(stamp + t, id) == id) return;
-  if (!wq) {
-    list[atomicAdd(cnt, 1)] = t;
-  } else if (!wq_push(*wq, t)) {
-    raise_error(P, CGC_ERR_TIMEOUT);
-  }
-}
 
 // block-wide int64 sum (512 threads); result valid in thread 0
 __device__ __forceinline__ long long block_sum64(long long v, long long* red) {
@@ -182,7 +170,7 @@ template <bool APPEND>
 __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
-                           const SweepExtra ex = SweepExtra(), const WorkQueue* wq = nullptr) {
+                           const SweepExtra ex = SweepExtra()) {
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -337,18 +325,14 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
     if (ex.tr_pulses && ex.tr_pulses[t] == 0) ex.tr_pulses[t] = (uint8_t)(S.lastout > 0 ? min(S.lastout, 254) : 255);
     atomicAdd(P.stats + S_TILES_SWEPT, 1ull);
     atomicAdd(P.stats + S_PULSES, (unsigned long long)pulses);
-    // work queue: release the tile first, so that the tiles queued below can be
-    // locked as soon as they are taken
-    if (wq) tile_unlock(P, t);
   }
-  if (wq) __syncthreads();
   // the tile re-queues itself from another warp than thread 0's face chain,
   // so the two dependent atomic chains overlap
-  if (APPEND && l == 32 && still) enqueue(P, P.stamp_sw, t, id_self, list_self, cnt_self, wq);
+  if (APPEND && l == 32 && still) queue_tile(P, P.stamp_sw, t, id_self, list_self, cnt_self);
   if (l < 6 && ((S.flags >> l) & 1)) {
     const int nt = S.nb[l];
     P.act[nt] = 1;
-    if (APPEND) enqueue(P, P.stamp_sw, nt, id_next, list_next, cnt_next, wq);
+    if (APPEND) queue_tile(P, P.stamp_sw, nt, id_next, list_next, cnt_next);
   }
   __syncthreads();
 }
@@ -434,13 +418,8 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
 // until the tile is stable; re-queue face neighbours whose halo changed.
-//
-// Work queue: a tile may be visited by two CTAs at once (it was queued again
-// while being visited).  Heights then only go down through atomicMin, and
-// the active flag is only ever set here (bfs_init_tile clears it): both
-// results are the ones of the visit that read the freshest halo.
 __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
-                         int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
+                         int32_t* list_next, int32_t* cnt_next) {
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
   const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
@@ -468,17 +447,16 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
     if (!any) break;
   }
   if (h < h0) {
-    const bool lowered = wq ? atomicMin(P.h + g, h) > h : true;
-    if (!wq) P.h[g] = h;
+    P.h[g] = h;
     const int fb = face_bits(x, y, z);
-    if (fb && lowered) atomicOr(&S.flags, fb);
+    if (fb) atomicOr(&S.flags, fb);
   }
   const int act = __syncthreads_or(has_excess && h < INF);
   if (l == 0) {
     if (act) P.act[t] = 1;
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
   }
-  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) enqueue(P, P.stamp_bfs, nb, id_next, list_next, cnt_next, wq);
+  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) queue_tile(P, P.stamp_bfs, nb, id_next, list_next, cnt_next);
   __syncthreads();
 }
 
@@ -487,7 +465,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
 // closure of {v : e(v) > 0} over residual edges, seeded by reach_init_tile_w
 // (a warp per tile).
 __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
-                           int32_t* list_next, int32_t* cnt_next, const WorkQueue* wq = nullptr) {
+                           int32_t* list_next, int32_t* cnt_next) {
   const int l = threadIdx.x;
   const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
@@ -530,7 +508,7 @@ __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S,
     if (fb) atomicOr(&S.flags, fb);
   }
   __syncthreads();
-  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) enqueue(P, P.stamp_bfs, nb, id_next, list_next, cnt_next, wq);
+  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) queue_tile(P, P.stamp_bfs, nb, id_next, list_next, cnt_next);
   __syncthreads();
 }
 

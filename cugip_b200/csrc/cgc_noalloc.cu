@@ -31,6 +31,7 @@
 #include "cgc.h"
 #include "cgc_internal.h"
 #include "cgc_device.cuh"
+#include "cgc_pool.h"
 
 namespace cgc {
 namespace {
@@ -186,17 +187,10 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   k_prepare<<<(unsigned)T, 512, 0, st>>>(P);
   NA_CUDA(cudaGetLastError());
 
-  cgc_options o{};
-  if (opts) o = *opts;
-  SolveParams prm;
-  prm.L = o.local_pulses > 0 ? (o.local_pulses < 64 ? o.local_pulses : 64) : 4;
-  prm.R = o.region_relabels < 0 ? 0 : (o.region_relabels > 0 ? (o.region_relabels < 16 ? o.region_relabels : 16) : 2);
-  prm.K = o.sweeps_per_relabel > 0 ? o.sweeps_per_relabel : 8;
-  prm.stall = o.stall_sweeps > 0 ? o.stall_sweeps : 0;
-  prm.learned = 0;       // the learned scheduler needs allocated buffers
-  prm.trace_cycles = 0;
-  prm.max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : (1 << 17);
-  prm.limit_ns = 20ull * 1000000000ull;
+  cgc_options o = resolve_options(opts);
+  o.learned = 0;  // the learned scheduler and its traces need allocated buffers
+  o.trace_cycles = 0;
+  const SolveParams prm = solve_params(o);
   void* args[] = {(void*)&P, (void*)&prm};
   // a preparation error (overflowing capacities) makes every CTA leave at its
   // first barrier

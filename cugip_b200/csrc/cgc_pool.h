@@ -50,7 +50,6 @@ struct Pool {
   int coop_blocks = 0;           // co-resident CTAs of k_solve
   int coop_blocks3 = 0;          // co-resident CTAs of k_solve3
   int coop_blocks4 = 0;          // co-resident CTAs of k_solve4
-  int coop_blocks_w = 0;         // co-resident CTAs of k_solve_w
   int sweep_blocks = 0;
   cgc_stats st{};
   std::vector<int64_t> flows;
@@ -96,6 +95,8 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out);
 int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT, bool host);
 int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32_t* bwd, bool host);
 cgc_options resolve_options(const cgc_options* o);
+uint64_t wait_limit_ns(const cgc_options& o);
+SolveParams solve_params(const cgc_options& o);
 int pool_solve(Pool& p, const cgc_options* opts);
 // cooperative launch of the persistent solve kernel selected by the options
 int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream);

@@ -53,41 +53,36 @@ def _ptr(a: np.ndarray):
 
 
 class Policy:
-    """Runtime counterpart of GraphCutPolicy (detail/graph_cut_policies.hpp:23-89)."""
+    """Runtime counterpart of GraphCutPolicy (detail/graph_cut_policies.hpp:23-89).
 
-    def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, schedule: int = 0,
+    Every field is a cgc_options field (include/cgc.h); 0 means the default."""
+
+    def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, wait_limit_us: int = 0,
                  max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0,
-                 ctas_per_sm: int = 0, learned: int = 0, trace_cycles: int = 0, warp_tiles: int = 0,
-                 bfs_warp_min: int = 0):
-        self.bfs_warp_min = bfs_warp_min
-        self.warp_tiles = warp_tiles
-        self.learned = learned
-        self.trace_cycles = trace_cycles
-        self.ctas_per_sm = ctas_per_sm
-        self.region_relabels = region_relabels
-        self.stall_sweeps = stall_sweeps
+                 ctas_per_sm: int = 0, learned: int = 0, trace_cycles: int = 0, bfs_warp_min: int = 0):
         self.local_pulses = local_pulses
         self.sweeps_per_relabel = sweeps_per_relabel
-        self.schedule = schedule
+        self.wait_limit_us = wait_limit_us
         self.max_sweeps = max_sweeps
         self.persistent = persistent
+        self.region_relabels = region_relabels
+        self.stall_sweeps = stall_sweeps
+        self.ctas_per_sm = ctas_per_sm
+        self.learned = learned
+        self.trace_cycles = trace_cycles
+        self.bfs_warp_min = bfs_warp_min
 
     def options(self) -> _lib.Options:
-        return _lib.options(self.local_pulses, self.sweeps_per_relabel, self.schedule, self.max_sweeps,
-                            self.persistent, self.region_relabels, self.stall_sweeps, self.ctas_per_sm,
-                            self.learned, self.trace_cycles, self.warp_tiles, self.bfs_warp_min)
+        return _lib.options(**{k: getattr(self, k) for k in _lib.OPTION_FIELDS})
 
     @classmethod
     def from_options(cls, o: _lib.Options) -> "Policy":
-        return cls(local_pulses=o.local_pulses, sweeps_per_relabel=o.sweeps_per_relabel, schedule=o.schedule,
-                   max_sweeps=o.max_sweeps, persistent=o.persistent, region_relabels=o.region_relabels,
-                   stall_sweeps=o.stall_sweeps, ctas_per_sm=o.ctas_per_sm, learned=o.learned,
-                   trace_cycles=o.trace_cycles, warp_tiles=o.warp_tiles, bfs_warp_min=o.bfs_warp_min)
+        return cls(**{k: getattr(o, k) for k in _lib.OPTION_FIELDS})
 
     def __repr__(self):
         return (f"Policy(L={self.local_pulses}, R={self.region_relabels}, K={self.sweeps_per_relabel}, "
                 f"ctas={self.ctas_per_sm}, stall={self.stall_sweeps}, learned={self.learned}, "
-                f"warp={self.warp_tiles}, bfsw={self.bfs_warp_min})")
+                f"bfsw={self.bfs_warp_min})")
 
     def with_(self, **kw) -> "Policy":
         p = Policy.from_options(self.options())

@@ -58,14 +58,6 @@ enum {
   CGC_SEG_SOURCE_MIN = 1
 };
 
-/* schedules of the tile sweep */
-enum {
-  CGC_SCHED_PARITY = 0, /* checkerboard tiles: halo heights exact, deterministic */
-  CGC_SCHED_ASYNC = 1   /* work queue: tiles visited as soon as no face neighbour is
-                           being visited (tile locks), BFS label-correcting; no grid
-                           barrier per sweep or BFS round (persistent solve only) */
-};
-
 /* Solver options; zero-initialise and set struct_size = sizeof(cgc_options).
    A zero field means "use the default".  Replaces the compile-time policies
    GraphCutPolicy / RelabelPolicy / PushPolicy
@@ -74,18 +66,19 @@ typedef struct cgc_options {
   int32_t struct_size;
   int32_t local_pulses;       /* push/relabel pulses per region-relabel round (1..64), default 4 */
   int32_t sweeps_per_relabel; /* sweep pairs between global relabels, default 8 */
-  int32_t schedule;           /* CGC_SCHED_* (default parity) */
-  int32_t max_sweeps;         /* safety cap on sweeps, default 1<<17 */
+  int32_t wait_limit_us;      /* bound of every device-side wait (grid barriers of the persistent
+                                 solve), in microseconds; default 20 s.  A wait that runs out ends
+                                 the solve with CGC_ERR_TIMEOUT; the handle stays usable */
+  int32_t max_sweeps;         /* safety cap on sweeps, default 1<<17; CGC_ERR_NOT_CONVERGED when reached */
   int32_t persistent;         /* 1 = one cooperative launch per solve (default), -1 = host loop */
   int32_t region_relabels;    /* region-relabel rounds per tile visit (default 2, -1 = none) */
   int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
   int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers), 3 (40) or 4 (32 registers) */
   int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only */
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
-  int32_t warp_tiles;         /* persistent: 1 = one warp per tile visit (ten warps per SM), 0 = one 512-thread CTA */
   int32_t bfs_warp_min;       /* persistent, 3 or 4 CTAs/SM: BFS rounds with at least this many tiles per CTA
                                  visit a tile with one warp (0 = never, the default) */
-  int32_t reserved[3];
+  int32_t reserved[4];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */

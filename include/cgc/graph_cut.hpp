@@ -54,12 +54,11 @@ struct GraphCutPolicy {
   int region_relabels = 0;     // region relabels per tile visit (-1: none)
   int sweeps_per_relabel = 0;  // sweep pairs between exact global relabels
   int persistent = 0;          // 1: one cooperative launch, -1: host loop
-  int schedule = 0;            // CGC_SCHED_PARITY (default) or CGC_SCHED_ASYNC
+  int wait_limit_us = 0;       // bound of every device-side wait in microseconds (0: 20 s)
   int max_sweeps = 0;          // safety cap (0: default)
   int stall_sweeps = 0;        // relabel early after this many idle sweep pairs (0: never)
   int ctas_per_sm = 0;         // 2 (default), 3 or 4 CTAs per SM
   int learned = 0;             // learned scheduler: 1 budgets + priorities, 2 budgets only
-  int warp_tiles = 0;          // 1: one warp per tile visit
   int bfs_warp_min = 0;        // 3/4 CTAs per SM: BFS rounds with this many tiles per CTA use a warp per tile
   cgc_options options() const {
     cgc_options o{};
@@ -68,12 +67,11 @@ struct GraphCutPolicy {
     o.region_relabels = region_relabels;
     o.sweeps_per_relabel = sweeps_per_relabel;
     o.persistent = persistent;
-    o.schedule = schedule;
+    o.wait_limit_us = wait_limit_us;
     o.max_sweeps = max_sweeps;
     o.stall_sweeps = stall_sweeps;
     o.ctas_per_sm = ctas_per_sm;
     o.learned = learned;
-    o.warp_tiles = warp_tiles;
     o.bfs_warp_min = bfs_warp_min;
     return o;
   }
@@ -87,12 +85,11 @@ struct GraphCutPolicy {
     out->region_relabels = o.region_relabels;
     out->sweeps_per_relabel = o.sweeps_per_relabel;
     out->persistent = o.persistent;
-    out->schedule = o.schedule;
+    out->wait_limit_us = o.wait_limit_us;
     out->max_sweeps = o.max_sweeps;
     out->stall_sweeps = o.stall_sweeps;
     out->ctas_per_sm = o.ctas_per_sm;
     out->learned = o.learned;
-    out->warp_tiles = o.warp_tiles;
     out->bfs_warp_min = o.bfs_warp_min;
     return true;
   }

@@ -140,8 +140,8 @@ int main() {
     cgc::GraphCutPolicy pols[6];
     pols[0].ctas_per_sm = 3; pols[0].bfs_warp_min = 1;
     pols[1].ctas_per_sm = 4; pols[1].region_relabels = 4; pols[1].local_pulses = 2;
-    pols[2].schedule = CGC_SCHED_ASYNC;
-    pols[3].warp_tiles = 1;
+    pols[2].ctas_per_sm = 4; pols[2].bfs_warp_min = 8;
+    pols[3].region_relabels = -1; pols[3].local_pulses = 8;
     pols[4].persistent = -1; pols[4].sweeps_per_relabel = 4;
     pols[5].stall_sweeps = 2; pols[5].ctas_per_sm = 3;
     for (const auto& p : pols) EXPECT(solve(&p) == f0);

@@ -53,9 +53,8 @@ def test_ctypes_mirrors_match_the_c_structs(tmp_path):
 
 
 def test_python_policy_round_trip_keeps_every_field():
-    values = dict(local_pulses=3, sweeps_per_relabel=5, schedule=1, max_sweeps=77, persistent=-1,
-                  region_relabels=2, stall_sweeps=4, ctas_per_sm=3, learned=2, trace_cycles=6, warp_tiles=1,
-                  bfs_warp_min=8)
+    values = dict(local_pulses=3, sweeps_per_relabel=5, wait_limit_us=1000, max_sweeps=77, persistent=-1,
+                  region_relabels=2, stall_sweeps=4, ctas_per_sm=3, learned=2, trace_cycles=6, bfs_warp_min=8)
     p = Policy(**values)
     o = p.options()
     assert o.struct_size == C.sizeof(_lib.Options)
@@ -75,18 +74,18 @@ CPP = r"""
 
 int main() {
   cgc::GraphCutPolicy p;
-  p.local_pulses = 3; p.region_relabels = 2; p.sweeps_per_relabel = 5; p.persistent = -1; p.schedule = 1;
-  p.max_sweeps = 77; p.stall_sweeps = 4; p.ctas_per_sm = 3; p.learned = 2; p.warp_tiles = 1; p.bfs_warp_min = 8;
+  p.local_pulses = 3; p.region_relabels = 2; p.sweeps_per_relabel = 5; p.persistent = -1; p.wait_limit_us = 1000;
+  p.max_sweeps = 77; p.stall_sweeps = 4; p.ctas_per_sm = 3; p.learned = 2; p.bfs_warp_min = 8;
   const cgc_options o = p.options();
   EXPECT(o.struct_size == (int)sizeof(cgc_options));
   EXPECT(o.local_pulses == 3 && o.region_relabels == 2 && o.sweeps_per_relabel == 5 && o.persistent == -1);
-  EXPECT(o.schedule == 1 && o.max_sweeps == 77 && o.stall_sweeps == 4 && o.ctas_per_sm == 3);
-  EXPECT(o.learned == 2 && o.warp_tiles == 1 && o.bfs_warp_min == 8 && o.trace_cycles == 0);
+  EXPECT(o.wait_limit_us == 1000 && o.max_sweeps == 77 && o.stall_sweeps == 4 && o.ctas_per_sm == 3);
+  EXPECT(o.learned == 2 && o.bfs_warp_min == 8 && o.trace_cycles == 0);
   // the cache file holds one choice for a single 256^3 grid
   cgc::GraphCutPolicy t;
   EXPECT(cgc::GraphCutPolicy::autotuned(256LL * 256 * 256, 1, &t));
   EXPECT(t.local_pulses == 4 && t.region_relabels == 2 && t.sweeps_per_relabel == 8);
-  EXPECT(t.ctas_per_sm == 3 && t.bfs_warp_min == 8 && t.stall_sweeps == 0 && t.warp_tiles == 0);
+  EXPECT(t.ctas_per_sm == 3 && t.bfs_warp_min == 8 && t.stall_sweeps == 0 && t.learned == 0);
   // no entry for another size class
   cgc::GraphCutPolicy u;
   EXPECT(!cgc::GraphCutPolicy::autotuned(64LL * 64 * 64, 1, &u));
@@ -104,7 +103,7 @@ def test_cpp_policy_fills_every_option_and_reads_the_autotune_cache(tmp_path):
     exe = str(tmp_path / "policy")
     subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", INCLUDE, str(src), "-L", LIBDIR,
                     "-lcgc", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
-    # size class of one 256^3 instance: (0, floor(2 log2 N)); fields L R K ctas stall warp bfs_warp_min ms
+    # size class of one 256^3 instance: (0, floor(2 log2 N)); fields L R K ctas stall learned bfs_warp_min ms
     vb = math.floor(2 * math.log2(256 ** 3))
     cache = tmp_path / "autotune.cache"
     cache.write_text(f"0 {vb} 4 2 8 3 0 0 8 7.5\n")

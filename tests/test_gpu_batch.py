@@ -53,7 +53,9 @@ def test_enqueue_matches_golden(device_batch):
 
 
 @pytest.mark.parametrize("policy", [Policy(), Policy(local_pulses=2, region_relabels=4, sweeps_per_relabel=4, ctas_per_sm=3),
-                                    Policy(warp_tiles=1), Policy(schedule=1), Policy(ctas_per_sm=4, region_relabels=4),
+                                    Policy(ctas_per_sm=3, stall_sweeps=1, sweeps_per_relabel=64),
+                                    Policy(ctas_per_sm=4, region_relabels=-1, local_pulses=8),
+                                    Policy(ctas_per_sm=4, region_relabels=4),
                                     Policy(ctas_per_sm=4, region_relabels=4, bfs_warp_min=8)])
 def test_graph_replay_matches_golden(device_batch, policy):
     B, vols, ins, outs, flows = device_batch
@@ -197,3 +199,35 @@ def test_outputs_at_unaligned_addresses(device_batch, offset):
         assert sha(buf[offset:offset + v.N].cpu().numpy()) == CASES[KEYS[0]]["treach_sha256"]
     finally:
         G.close()
+
+
+@pytest.mark.parametrize("policy", [None, Policy(local_pulses=2, region_relabels=4, sweeps_per_relabel=4, ctas_per_sm=4,
+                                                 bfs_warp_min=8)])
+def test_all_96_instances_match_the_oracle(policy):
+    """The batched configuration itself: all 96 instances (extents 32..160)
+    bound to one batch, the CUDA graph replayed twice, and every instance's
+    flow and both cut sets compared with the oracle's golden answer."""
+    import torch
+    keys = [(4, i) for i in range(96)]
+    vols = [volume.workload(*k) for k in keys]
+    dev = torch.device("cuda", 0)
+    ins = [[torch.from_numpy(a).to(dev) for a in v.arrays()] for v in vols]
+    outs = [torch.full((2, v.N), 7, dtype=torch.uint8, device=dev) for v in vols]
+    B = Batch([(v.X, v.Y, v.Z) for v in vols])
+    try:
+        for i, (d, o) in enumerate(zip(ins, outs)):
+            B.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
+            B.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
+        B.graph_create(policy)
+        for rep in range(2):
+            for o in outs:
+                o.fill_(7)
+            B.graph_launch()
+            fl = B.wait()
+            for i, k in enumerate(keys):
+                c = CASES[k]
+                assert fl[i] == c["flow"], k
+                assert sha(outs[i][0].cpu().numpy()) == c["smin_sha256"], k
+                assert sha(outs[i][1].cpu().numpy()) == c["treach_sha256"], k
+    finally:
+        B.close()
