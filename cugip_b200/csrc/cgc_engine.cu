@@ -883,6 +883,10 @@ int pool_solve(Pool& p, const cgc_options* opts) {
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, p.stream));
   k_prepare<<<d.T, 512, 0, p.stream>>>(d); note_launch();
+  // from here on the planes hold the preflow, not the capacities: whatever
+  // the outcome, another solve needs new set_* calls
+  for (auto& u : p.uploaded) u = 0;
+  p.solved = false;
   CGC_CUDA(cudaGetLastError());
   int rc = check_device_error(p, "maxflow");
   auto destroy_events = [&]() { cudaEventDestroy(ev0); cudaEventDestroy(ev1); cudaEventDestroy(evk0); cudaEventDestroy(evk1); };

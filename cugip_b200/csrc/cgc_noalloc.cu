@@ -16,7 +16,11 @@
 //     CGC_ERR_ARG before anything is launched;
 //   * the first call on a device sets that device up (looks up the array's
 //     device address with cudaGetSymbolAddress and sizes the cooperative
-//     launch); make that first call before any stream capture;
+//     launch); make that first call before any stream capture.  The address
+//     is kept for the life of the process, so a cudaDeviceReset after the
+//     first call on a device is not supported;
+//   * every call blocks the calling thread: it reads the flow and the device
+//     status back into host memory and waits for the stream;
 //   * every call shares the one array, which keeps the previous call's
 //     contents; the call clears everything that must start at zero.  Calls
 //     that overlap on the GPU (from several host threads or streams) race on

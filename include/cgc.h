@@ -208,8 +208,13 @@ int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count);
  * this library holds until exit, so the grid may hold at most
  * CGC_NOALLOC_MAX_VOXELS voxels after rounding each extent up to a multiple of
  * 8 (64^3 fits); larger grids return CGC_ERR_ARG.  The first call on a device
- * sets that device up and should come before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race and must not be issued. */
+ * sets that device up and should come before any stream capture: it looks up
+ * the array's device address, which is then kept for the life of the process,
+ * so resetting the device (cudaDeviceReset) after that first call is not
+ * supported.  Every call blocks the calling thread: it waits for `stream` and
+ * reads the flow and the device status back into host memory before it
+ * returns.  Calls share the array: calls that overlap on the GPU race and must
+ * not be issued. */
 #define CGC_NOALLOC_MAX_VOXELS 262144
 int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const int32_t* capS, const int32_t* capT,
                              const int32_t* const fwd[3], const int32_t* const bwd[3],
