@@ -86,6 +86,10 @@ SIGNATURES = {
     "cgc_grid_set_tlinks_device": (C.c_int, [VP, VP, VP]),
     "cgc_grid_set_nlinks_device": (C.c_int, [VP, C.c_int, VP, VP]),
     "cgc_grid_maxflow": (C.c_int, [VP, C.POINTER(Options), P64]),
+    "cgc_grid_maxflow_async": (C.c_int, [VP, C.POINTER(Options)]),
+    "cgc_grid_get_labels": (C.c_int, [VP, VP]),
+    "cgc_graph_get_state": (C.c_int, [VP, VP, VP]),
+    "cgc_grid_wait": (C.c_int, [VP, P64]),
     "cgc_grid_get_segments": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
     "cgc_grid_get_segments_device": (C.c_int, [VP, C.c_int, VP, C.c_uint8, C.c_uint8]),
     "cgc_grid_get_residuals": (C.c_int, [VP, C.POINTER(VP), VP, VP]),

@@ -111,25 +111,15 @@ int pool_autotune(Pool& p, const cgc_options* cands, int32_t n, int32_t repeats,
   std::vector<cgc_options> cand = (cands && n > 0) ? std::vector<cgc_options>(cands, cands + n) : default_candidates();
   if (repeats <= 0) repeats = 1;
   const bool bound = inputs_bound(p);
-  void* snap = nullptr;
-  const size_t plane = (size_t)p.Np * 4;
-  if (!bound) {
+  if (p.pending) return fail(CGC_ERR_STATE, "autotune: a solve of this handle was not waited for");
+  if (!bound)
     for (int i = 0; i < p.ninst; ++i)
       if (!(p.uploaded[i] & 1u)) return fail(CGC_ERR_STATE, "autotune: set the capacities (or bind device inputs) first");
-    CGC_CUDA(cudaMalloc(&snap, 8 * plane));
-    char* sp = (char*)snap;
-    CGC_CUDA(cudaMemcpyAsync(sp, p.dp.e, plane, cudaMemcpyDeviceToDevice, p.stream));
-    CGC_CUDA(cudaMemcpyAsync(sp + plane, p.dp.rT, plane, cudaMemcpyDeviceToDevice, p.stream));
-    CGC_CUDA(cudaMemcpyAsync(sp + 2 * plane, p.dp.r, 6 * plane, cudaMemcpyDeviceToDevice, p.stream));
-  }
+  // the set_* inputs stay in their linear planes through a solve: marking
+  // them as set again restores them
   const std::vector<uint32_t> uploaded = p.uploaded;
   auto restore = [&]() -> int {
-    if (bound) return CGC_OK;
-    char* sp = (char*)snap;
-    CGC_CUDA(cudaMemcpyAsync(p.dp.e, sp, plane, cudaMemcpyDeviceToDevice, p.stream));
-    CGC_CUDA(cudaMemcpyAsync(p.dp.rT, sp + plane, plane, cudaMemcpyDeviceToDevice, p.stream));
-    CGC_CUDA(cudaMemcpyAsync(p.dp.r, sp + 2 * plane, 6 * plane, cudaMemcpyDeviceToDevice, p.stream));
-    p.uploaded = uploaded;
+    if (!bound) p.uploaded = uploaded;
     return CGC_OK;
   };
   cudaEvent_t e0, e1;
@@ -161,7 +151,6 @@ int pool_autotune(Pool& p, const cgc_options* cands, int32_t n, int32_t repeats,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   int rc2 = restore();
-  if (snap) cudaFree(snap);
   if (rc) return rc;
   if (rc2) return rc2;
   if (best_i < 0) return fail(CGC_ERR_STATE, "autotune: every candidate failed");

@@ -572,7 +572,11 @@ int graph_maxflow(cgc_graph* g, const cgc_options* opts, int64_t* flow) {
     cfg.stream = g->stream;
     cfg.gridDim = dim3(g->coop_blocks);
     cfg.blockDim = dim3(CSR_THREADS);
-    CGC_CUDA(cudaLaunchKernelEx(&cfg, k_csr_solve, d, prm));
+    if (int rc2 = coop_launch_ordered(g->device, g->stream, [&]() -> int {
+          CGC_CUDA(cudaLaunchKernelEx(&cfg, k_csr_solve, d, prm));
+          return CGC_OK;
+        }))
+      return rc2;
     note_launch();
     CGC_CUDA(cudaEventRecord(ev[2], g->stream));
     CGC_CUDA(cudaEventRecord(ev[3], g->stream));
@@ -648,6 +652,18 @@ int cgc_graph_get_segments(cgc_graph* g, int which, uint8_t* out, uint8_t mask, 
   CGC_CUDA(cudaGetLastError());
   CGC_CUDA(cudaMemcpyAsync(out, g->seg, (size_t)g->n, cudaMemcpyDeviceToHost, g->stream));
   CGC_CUDA(cudaStreamSynchronize(g->stream));
+  return cgc::ok();
+}
+
+int cgc_graph_get_state(cgc_graph* g, int32_t* labels, int32_t* excess) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "cgc_graph_get_state: null graph");
+  if (!g->solved) return cgc::fail(CGC_ERR_STATE, "cgc_graph_get_state: call maxflow first");
+  if (labels) CGC_CUDA(cudaMemcpyAsync(labels, g->d.h, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
+  if (excess) CGC_CUDA(cudaMemcpyAsync(excess, g->d.e, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
+  CGC_CUDA(cudaStreamSynchronize(g->stream));
+  if (labels)
+    for (int32_t v = 0; v < g->n; ++v)
+      if (labels[v] >= cgc::INF) labels[v] = INT32_MIN;
   return cgc::ok();
 }
 

@@ -50,7 +50,8 @@ enum Stat {
 
 // phase trace records written by the persistent solve (two words each):
 //   word 0 = kind << 56 | index << 24 | tiles, word 1 = ns since the launch
-enum TraceKind { TR_BFS_ROUND = 1, TR_RELABEL_DONE = 2, TR_SWEEP = 3, TR_REACH_ROUND = 4 };
+//   (TR_FLOW: word 1 = the flow delivered so far, all instances together)
+enum TraceKind { TR_BFS_ROUND = 1, TR_RELABEL_DONE = 2, TR_SWEEP = 3, TR_REACH_ROUND = 4, TR_FLOW = 5 };
 constexpr int TRACE_CAP = 16384;
 
 // BFS seed summary of a tile (DevPool::tflag)
@@ -130,5 +131,8 @@ __global__ void k_solve4(DevPool P, SolveParams prm);
 __global__ void k_solve3w(DevPool P, SolveParams prm);
 __global__ void k_solve4w(DevPool P, SolveParams prm);
 __global__ void k_segments(DevPool P, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg);
+// kernels of cgc_batch.cu
+__global__ void k_put_all(DevPool P, const int32_t* const* __restrict__ in);
+__global__ void k_seg_all(DevPool P, uint8_t* const* __restrict__ out);
 
 }  // namespace cgc

@@ -15,7 +15,9 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -149,13 +151,38 @@ __global__ void __launch_bounds__(512) k_prepare(DevPool P) {
   }
 }
 
-__global__ void k_zero_axis(DevPool P, int inst, int axis) {
-  const InstGeo G = P.geo[inst];
-  const int64_t n = (int64_t)G.TX * G.TY * G.TZ * TV;
-  const int64_t base = (int64_t)G.tile_base * TV;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    P.r[(2 * axis) * P.Np + base + i] = 0;
-    P.r[(2 * axis + 1) * P.Np + base + i] = 0;
+// Fused upload + preflow of a single instance whose 8 input planes (capS,
+// capT, fwd x/y/z, bwd x/y/z; null = zero) are passed by value, so a queued
+// solve reads exactly the planes of its own set_* calls (put_tile4).
+struct InputPlanes { const int32_t* p[8]; };
+__global__ void __launch_bounds__(128) k_put_one(DevPool P, InputPlanes in) {
+  put_tile4(P, blockIdx.x, in.p);
+}
+
+// Cut sets as mask / background bytes from the 1/0 bytes of one buffer
+// (16 bytes per thread where src and dst allow it).
+__global__ void k_mask_remap(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int64_t n, uint8_t mask,
+                             uint8_t bg) {
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (vec) {
+    const int64_t n16 = n / 16;
+    for (int64_t i = i0; i < n16; i += stride) {
+      uint4 v = reinterpret_cast<const uint4*>(src)[i];
+      unsigned* w = reinterpret_cast<unsigned*>(&v);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        unsigned o = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) o |= (unsigned)(((w[k] >> (8 * b)) & 1u) ? mask : bg) << (8 * b);
+        w[k] = o;
+      }
+      reinterpret_cast<uint4*>(dst)[i] = v;
+    }
+    for (int64_t i = n16 * 16 + i0; i < n; i += stride) dst[i] = src[i] ? mask : bg;
+  } else {
+    for (int64_t i = i0; i < n; i += stride) dst[i] = src[i] ? mask : bg;
   }
 }
 
@@ -392,6 +419,13 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     if (!grid_sync(P, prm.limit_ns)) return;
     const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));
     record(TR_RELABEL_DONE, relabels, nact);
+    if (b == 0 && tid == 0 && P.trace && ntrace < TRACE_CAP) {  // flow at this relabel (after the barrier)
+      unsigned long long f = 0;
+      for (int i = 0; i < P.ninst; ++i) f += __ldcg(P.flow + i);
+      P.trace[2 * ntrace] = ((unsigned long long)TR_FLOW << 56) | ((unsigned long long)(relabels & 0xffffffffll) << 24);
+      P.trace[2 * ntrace + 1] = f;
+      ++ntrace;
+    }
     if (nact == 0) break;
     if (sweeps >= prm.max_sweeps) {
       if (b == 0 && tid == 0) raise_error(P, CGC_ERR_NOT_CONVERGED);
@@ -485,6 +519,28 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   }
 }
 
+// Cooperative launches of this library on one device run one after another.
+// Each waits on the device (an event, no host synchronisation) for the
+// previous one to end: two grid-barrier kernels in flight on different
+// streams could each hold part of the SMs and wait for their missing CTAs,
+// until their bounded barriers gave up.  Launches into a stream under capture
+// are not ordered (a CUDA graph is replayed on its own).
+static std::mutex g_coop_mu;
+static cudaEvent_t g_coop_last[64] = {};
+
+int coop_launch_ordered(int device, cudaStream_t stream, const std::function<int()>& launch) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CGC_CUDA(cudaStreamIsCapturing(stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone || device < 0 || device >= 64) return launch();
+  std::lock_guard<std::mutex> lock(g_coop_mu);
+  cudaEvent_t& last = g_coop_last[device];
+  if (!last) CGC_CUDA(cudaEventCreateWithFlags(&last, cudaEventDisableTiming));
+  CGC_CUDA(cudaStreamWaitEvent(stream, last, 0));  // a no-op before the first record
+  if (int rc = launch()) return rc;
+  CGC_CUDA(cudaEventRecord(last, stream));
+  return CGC_OK;
+}
+
 int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -498,9 +554,13 @@ int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolvePar
   cfg.blockDim = dim3(512);
   cfg.dynamicSmemBytes = 0;
   const bool bw = prm.bfs_warp_min > 0;
-  if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve4w : k_solve4, d, prm));
-  else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve3w : k_solve3, d, prm));
-  else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
+  int rc = coop_launch_ordered(p.device, stream, [&]() -> int {
+    if (four) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve4w : k_solve4, d, prm));
+    else if (three) CGC_CUDA(cudaLaunchKernelEx(&cfg, bw ? k_solve3w : k_solve3, d, prm));
+    else CGC_CUDA(cudaLaunchKernelEx(&cfg, k_solve, d, prm));
+    return CGC_OK;
+  });
+  if (rc) return rc;
   note_launch();
   return ok();
 }
@@ -678,9 +738,15 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   CGC_CUDA(cudaMemcpyAsync((void*)d.tinst, ti.data(), ti.size() * 4, cudaMemcpyHostToDevice, p->stream));
   CGC_CUDA(cudaMemcpyAsync((void*)d.tpar, tp.data(), tp.size(), cudaMemcpyHostToDevice, p->stream));
   CGC_CUDA(cudaMemcpyAsync((void*)d.geo, p->geo.data(), p->geo.size() * sizeof(InstGeo), cudaMemcpyHostToDevice, p->stream));
-  CGC_CUDA(cudaMalloc(&p->staging, 2 * p->maxN * 4));
-  CGC_CUDA(cudaMalloc(&p->seg, p->maxN));
+  p->voff.resize(count);
+  for (int i = 0; i < count; ++i) {
+    p->voff[i] = p->sumN;
+    p->sumN += (int64_t)p->geo[i].X * p->geo[i].Y * p->geo[i].Z;
+  }
+  p->host_in.assign(8 * (size_t)count, nullptr);
   CGC_CUDA(cudaMallocHost(&p->pinned_cnt, 64 * 4));
+  CGC_CUDA(cudaEventCreateWithFlags(&p->inputs_read, cudaEventDisableTiming));
+  for (auto& e : p->ev) CGC_CUDA(cudaEventCreate(&e));
 
   cudaDeviceProp prop;
   CGC_CUDA(cudaGetDeviceProperties(&prop, p->device));
@@ -705,39 +771,29 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   return ok();
 }
 
-// Host upload of one or two planes into the next of the two staging buffers,
-// on a copy stream of its own.  Returns once the host arrays have been read,
-// which is the setters' contract (the caller may reuse them at once, pinned or
-// not).  The permute kernel that follows runs on the solve stream while the
-// next upload already copies into the other buffer; a buffer is overwritten
-// only after the kernel that read it (event `consumed`, recorded by
-// stage_done).
-static int stage_upload(Pool& p, const int32_t* a, const int32_t* b, int64_t N, const int32_t** da,
-                        const int32_t** db) {
-  if (!p.copy_stream) {
+// Inputs of the set_* calls go into linear device planes (one copy per
+// plane, no kernel); the fused upload kernel of the next solve reads them.
+// Host uploads run on a copy stream of their own, after the upload kernel of
+// the last enqueued solve has read the planes (event inputs_read), and the
+// setter returns once the host array has been read: the reference's setters
+// copy at call time too (graph_cut.hpp:284-285, 298-299).  Device-pointer
+// setters copy device to device on the solve stream.
+static int ensure_lin(Pool& p, bool bwd) {
+  if (!p.lin) {
+    CGC_CUDA(cudaMalloc(&p.lin, 5 * (size_t)p.sumN * 4));
     CGC_CUDA(cudaStreamCreateWithFlags(&p.copy_stream, cudaStreamNonBlocking));
-    for (int k = 0; k < 2; ++k) {
-      CGC_CUDA(cudaEventCreateWithFlags(&p.staged[k], cudaEventDisableTiming));
-      CGC_CUDA(cudaEventCreateWithFlags(&p.consumed[k], cudaEventDisableTiming));
-    }
-    CGC_CUDA(cudaMalloc(&p.staging2, 2 * p.maxN * 4));
   }
-  const int k = p.stage;
-  int32_t* buf = k ? p.staging2 : p.staging;
-  CGC_CUDA(cudaStreamWaitEvent(p.copy_stream, p.consumed[k], 0));  // no-op before the first record
-  CGC_CUDA(cudaMemcpyAsync(buf, a, N * 4, cudaMemcpyHostToDevice, p.copy_stream));
-  if (b) CGC_CUDA(cudaMemcpyAsync(buf + p.maxN, b, N * 4, cudaMemcpyHostToDevice, p.copy_stream));
-  CGC_CUDA(cudaEventRecord(p.staged[k], p.copy_stream));
-  CGC_CUDA(cudaEventSynchronize(p.staged[k]));
-  *da = buf;
-  if (db) *db = b ? buf + p.maxN : nullptr;
+  if (bwd && !p.lin_bwd) CGC_CUDA(cudaMalloc(&p.lin_bwd, 3 * (size_t)p.sumN * 4));
   return CGC_OK;
 }
 
-// After the kernel that reads the current staging buffer was launched.
-static int stage_done(Pool& p) {
-  CGC_CUDA(cudaEventRecord(p.consumed[p.stage], p.stream));
-  p.stage ^= 1;
+static int copy_plane(Pool& p, int32_t* dst, const int32_t* src, int64_t N, bool host) {
+  if (host) {
+    CGC_CUDA(cudaStreamWaitEvent(p.copy_stream, p.inputs_read, 0));  // no-op before the first record
+    CGC_CUDA(cudaMemcpyAsync(dst, src, N * 4, cudaMemcpyHostToDevice, p.copy_stream));
+  } else {
+    CGC_CUDA(cudaMemcpyAsync(dst, src, N * 4, cudaMemcpyDeviceToDevice, p.stream));
+  }
   return CGC_OK;
 }
 
@@ -745,19 +801,17 @@ int pool_put_tlinks(Pool& p, int inst, const int32_t* capS, const int32_t* capT,
   if (inst < 0 || inst >= p.ninst || !capS || !capT) return fail(CGC_ERR_ARG, "set_tlinks: bad arguments");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
-  const int32_t *s = capS, *c = capT;
-  if (host) {
-    int rc = stage_upload(p, capS, capT, N, &s, &c);
-    if (rc) return rc;
-  }
-  k_put_tlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, s, c); note_launch();
-  CGC_CUDA(cudaGetLastError());
-  if (host) {
-    int rc = stage_done(p);
-    if (rc) return rc;
-  }
+  if (int rc = ensure_lin(p, false)) return rc;
+  int32_t* s = p.lin + p.voff[inst];
+  int32_t* c = p.lin + p.sumN + p.voff[inst];
+  if (int rc = copy_plane(p, s, capS, N, host)) return rc;
+  if (int rc = copy_plane(p, c, capT, N, host)) return rc;
+  if (host) CGC_CUDA(cudaStreamSynchronize(p.copy_stream));
+  p.host_in[8 * (size_t)inst] = s;
+  p.host_in[8 * (size_t)inst + 1] = c;
   p.uploaded[inst] |= 1u;
   p.solved = false;
+  p.seg_valid = false;
   return ok();
 }
 
@@ -766,21 +820,19 @@ int pool_put_nlinks(Pool& p, int inst, int axis, const int32_t* fwd, const int32
     return fail(CGC_ERR_ARG, "set_nlinks: bad arguments");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
-  const int32_t *f = fwd, *b = bwd;
-  if (host) {
-    const bool same = bwd == fwd;  // symmetric weights: one plane
-    int rc = stage_upload(p, fwd, same ? nullptr : bwd, N, &f, &b);
-    if (rc) return rc;
-    if (same) b = f;
-  }
-  k_put_nlinks<<<G.TX * G.TY * G.TZ, 512, 0, p.stream>>>(p.dp, inst, axis, f, b); note_launch();
-  CGC_CUDA(cudaGetLastError());
-  if (host) {
-    int rc = stage_done(p);
-    if (rc) return rc;
-  }
+  const bool same = bwd == fwd;  // symmetric weights: one plane
+  if (int rc = ensure_lin(p, !same)) return rc;
+  int32_t* f = p.lin + (2 + axis) * p.sumN + p.voff[inst];
+  int32_t* b = same ? f : p.lin_bwd + axis * p.sumN + p.voff[inst];
+  if (int rc = copy_plane(p, f, fwd, N, host)) return rc;
+  if (!same)
+    if (int rc = copy_plane(p, b, bwd, N, host)) return rc;
+  if (host) CGC_CUDA(cudaStreamSynchronize(p.copy_stream));
+  p.host_in[8 * (size_t)inst + 2 + axis] = f;
+  p.host_in[8 * (size_t)inst + 5 + axis] = b;
   p.uploaded[inst] |= 2u << axis;
   p.solved = false;
+  p.seg_valid = false;
   return ok();
 }
 
@@ -858,56 +910,85 @@ static int host_bfs(Pool& p, uint32_t& id, int64_t& rounds) {
   return CGC_OK;
 }
 
-int pool_solve(Pool& p, const cgc_options* opts) {
+// Buffers of the host-path outputs: both cut sets of every instance (1/0
+// bytes, linear order) and the device table of their addresses.
+static int ensure_segbuf(Pool& p) {
+  if (p.segbuf) return CGC_OK;
+  CGC_CUDA(cudaMalloc(&p.segbuf, 2 * (size_t)p.sumN));
+  CGC_CUDA(cudaMalloc(&p.d_segtab, 2 * (size_t)p.ninst * sizeof(uint8_t*)));
+  std::vector<uint8_t*> tab(2 * (size_t)p.ninst);
+  for (int i = 0; i < p.ninst; ++i) {
+    tab[2 * i] = p.segbuf + p.voff[i];               // source side
+    tab[2 * i + 1] = p.segbuf + p.sumN + p.voff[i];  // sink side
+  }
+  CGC_CUDA(cudaMemcpy(p.d_segtab, tab.data(), tab.size() * sizeof(uint8_t*), cudaMemcpyHostToDevice));
+  return CGC_OK;
+}
+
+// Enqueues one solve of the set_* inputs on p.stream: fused upload and
+// preflow, the solve, and both cut sets of every instance into segbuf.  With
+// the persistent solve (the default) nothing synchronises the host, so the
+// next grid's host uploads can run while this one solves; the host-driven
+// schedule (persistent = -1) runs its loop here.
+int pool_solve_async(Pool& p, const cgc_options* opts) {
+  if (p.pending) return fail(CGC_ERR_STATE, "maxflow: the previous solve of this handle was not waited for");
   const cgc_options o = resolve_options(opts);
   DevPool& d = p.dp;
-  for (int i = 0; i < p.ninst; ++i) {
+  for (int i = 0; i < p.ninst; ++i)
     if (!(p.uploaded[i] & 1u)) return fail(CGC_ERR_STATE, "maxflow: set_tlinks was not called since the last solve");
+  // axes not set since the last solve have zero capacity
+  std::vector<const int32_t*> in = p.host_in;
+  for (int i = 0; i < p.ninst; ++i)
     for (int a = 0; a < 3; ++a)
-      if (!(p.uploaded[i] & (2u << a))) {
-        const InstGeo& G = p.geo[i];
-        k_zero_axis<<<std::max(1, std::min(G.TX * G.TY * G.TZ, 1024)), 512, 0, p.stream>>>(d, i, a); note_launch();
-      }
+      if (!(p.uploaded[i] & (2u << a))) in[8 * (size_t)i + 2 + a] = in[8 * (size_t)i + 5 + a] = nullptr;
+  const SolveParams prm = solve_params(o);
+  if (o.persistent > 0 && (prm.learned || prm.trace_cycles))  // buffers and weights before anything is queued
+    if (int rc = ensure_sched(p, prm.learned != 0, prm.trace_cycles)) return rc;
+  if (int rc = ensure_segbuf(p)) return rc;
+  if (p.ninst > 1) {
+    if (!p.d_host_in) CGC_CUDA(cudaMalloc(&p.d_host_in, 8 * (size_t)p.ninst * sizeof(int32_t*)));
+    // pageable source: the table is staged before the call returns
+    CGC_CUDA(cudaMemcpyAsync(p.d_host_in, in.data(), in.size() * sizeof(int32_t*), cudaMemcpyHostToDevice, p.stream));
   }
-  const long long launches0 = g_launches.load();
-  cudaEvent_t ev0, ev1, evk0, evk1;
-  CGC_CUDA(cudaEventCreate(&ev0));
-  CGC_CUDA(cudaEventCreate(&ev1));
-  CGC_CUDA(cudaEventCreate(&evk0));
-  CGC_CUDA(cudaEventCreate(&evk1));
-  CGC_CUDA(cudaEventRecord(ev0, p.stream));
+  p.launches0 = g_launches.load();
+  CGC_CUDA(cudaEventRecord(p.ev[0], p.stream));
   CGC_CUDA(cudaMemsetAsync(d.flow, 0, (size_t)p.ninst * 8, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stats, 0, S_NSTATS * 8, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.err, 0, 4, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, p.stream));
-  k_prepare<<<d.T, 512, 0, p.stream>>>(d); note_launch();
-  // from here on the planes hold the preflow, not the capacities: whatever
-  // the outcome, another solve needs new set_* calls
+  if (p.ninst == 1) {
+    InputPlanes ip;
+    for (int k = 0; k < 8; ++k) ip.p[k] = in[k];
+    k_put_one<<<d.T, 128, 0, p.stream>>>(d, ip);
+  } else {
+    k_put_all<<<d.T, 128, 0, p.stream>>>(d, p.d_host_in);
+  }
+  note_launch();
+  CGC_CUDA(cudaGetLastError());
+  CGC_CUDA(cudaEventRecord(p.inputs_read, p.stream));  // the setters may overwrite the planes from here on
+  // the inputs are consumed: another solve needs new set_* calls
   for (auto& u : p.uploaded) u = 0;
   p.solved = false;
-  CGC_CUDA(cudaGetLastError());
-  int rc = check_device_error(p, "maxflow");
-  auto destroy_events = [&]() { cudaEventDestroy(ev0); cudaEventDestroy(ev1); cudaEventDestroy(evk0); cudaEventDestroy(evk1); };
-  if (rc) { destroy_events(); return rc; }
+  p.seg_valid = false;
+  p.pending = true;
+  p.pending_persistent = o.persistent;
 
-  int64_t sweeps = 0, relabels = 0, rounds = 0;
+  int rc = CGC_OK;
   if (o.persistent > 0) {
-    const SolveParams prm = solve_params(o);
-    if (prm.learned || prm.trace_cycles) {
-      rc = ensure_sched(p, prm.learned != 0, prm.trace_cycles);
-      if (rc) { destroy_events(); return rc; }
-    }
-    CGC_CUDA(cudaEventRecord(evk0, p.stream));
+    CGC_CUDA(cudaEventRecord(p.ev[2], p.stream));
     rc = launch_solve(p, o, d, prm, p.stream);
-    if (rc) { destroy_events(); return rc; }
-    CGC_CUDA(cudaEventRecord(evk1, p.stream));
+    CGC_CUDA(cudaEventRecord(p.ev[3], p.stream));
   } else {
-    CGC_CUDA(cudaEventRecord(evk0, p.stream));
+    // the host loop reads counters back every round; a preparation error
+    // (overflowing capacities) stops it before it starts
+    rc = check_device_error(p, "maxflow");
+    CGC_CUDA(cudaEventRecord(p.ev[2], p.stream));
+    int64_t sweeps = 0, relabels = 0, rounds = 0;
     uint32_t id = 1;
     int32_t* sl = d.lists + 3 * d.T;
-    for (;;) {
+    while (!rc) {
       rc = host_bfs<false>(p, id, rounds);
       if (rc) break;
       ++relabels;
@@ -930,75 +1011,117 @@ int pool_solve(Pool& p, const cgc_options* opts) {
       }
     }
     if (!rc) rc = host_bfs<true>(p, id, rounds);
-    CGC_CUDA(cudaEventRecord(evk1, p.stream));
+    CGC_CUDA(cudaEventRecord(p.ev[3], p.stream));
+    p.host_counts[0] = sweeps;
+    p.host_counts[1] = relabels;
+    p.host_counts[2] = rounds;
   }
-  CGC_CUDA(cudaEventRecord(ev1, p.stream));
-  if (!rc) rc = check_device_error(p, "maxflow");
-  float ms = 0.f, kms = 0.f;
   if (!rc) {
-    CGC_CUDA(cudaEventSynchronize(ev1));
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventElapsedTime(&kms, evk0, evk1);
+    const unsigned gx = (unsigned)std::min<int64_t>(std::max<int64_t>((p.maxN + 32767) / 32768, 1), 4096);
+    k_seg_all<<<dim3(gx, (unsigned)std::min(p.ninst, 65535)), 256, 0, p.stream>>>(d, p.d_segtab);
+    note_launch();
+    CGC_CUDA(cudaGetLastError());
   }
-  destroy_events();
-  if (rc) return rc;
+  CGC_CUDA(cudaEventRecord(p.ev[1], p.stream));
+  if (rc) {
+    // nothing to wait for: leave the stream idle and report now
+    cudaStreamSynchronize(p.stream);
+    p.pending = false;
+    return rc;
+  }
+  return ok();
+}
 
+// Waits for the solve enqueued by pool_solve_async; reports device errors and
+// reads the flows and statistics.
+int pool_solve_wait(Pool& p) {
+  if (!p.pending) return fail(CGC_ERR_STATE, "wait: no solve was enqueued");
+  p.pending = false;
+  CGC_CUDA(cudaEventSynchronize(p.ev[1]));
+  if (int rc = check_device_error(p, "maxflow")) return rc;
+  float ms = 0.f, kms = 0.f;
+  cudaEventElapsedTime(&ms, p.ev[0], p.ev[1]);
+  cudaEventElapsedTime(&kms, p.ev[2], p.ev[3]);
   unsigned long long stats[S_NSTATS];
-  CGC_CUDA(cudaMemcpy(stats, d.stats, sizeof(stats), cudaMemcpyDeviceToHost));
-  CGC_CUDA(cudaMemcpy(p.flows.data(), d.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToHost));
+  CGC_CUDA(cudaMemcpyAsync(stats, p.dp.stats, sizeof(stats), cudaMemcpyDeviceToHost, p.stream));
+  CGC_CUDA(cudaMemcpyAsync(p.flows.data(), p.dp.flow, (size_t)p.ninst * 8, cudaMemcpyDeviceToHost, p.stream));
+  CGC_CUDA(cudaStreamSynchronize(p.stream));
   std::memset(&p.st, 0, sizeof(p.st));
-  p.st.flow = 0;
   for (int64_t f : p.flows) p.st.flow += f;
-  if (o.persistent > 0) {
+  if (p.pending_persistent > 0) {
     p.st.sweeps = (int64_t)stats[S_SWEEPS];
     p.st.global_relabels = (int64_t)stats[S_RELABELS];
     p.st.bfs_rounds = (int64_t)stats[S_ROUNDS];
   } else {
-    p.st.sweeps = sweeps;
-    p.st.global_relabels = relabels;
-    p.st.bfs_rounds = rounds;
+    p.st.sweeps = p.host_counts[0];
+    p.st.global_relabels = p.host_counts[1];
+    p.st.bfs_rounds = p.host_counts[2];
   }
   p.st.tiles_swept = (int64_t)stats[S_TILES_SWEPT];
   p.st.tiles_relabelled = (int64_t)stats[S_TILES_BFS];
   p.st.pulses = (int64_t)stats[S_PULSES];
   p.st.solve_ms = ms;
   p.st.kernel_ms = kms;
-  p.st.launches = g_launches.load() - launches0;
+  p.st.launches = g_launches.load() - p.launches0;
   p.st.bfs_ms = 1e-6 * (double)stats[S_NS_BFS];
   p.st.sweep_ms = 1e-6 * (double)stats[S_NS_SWEEP];
   p.st.reach_ms = 1e-6 * (double)stats[S_NS_REACH];
   p.st.sched_ms = 1e-6 * (double)stats[S_NS_SCHED];
-  for (auto& u : p.uploaded) u = 0;
   p.solved = true;
+  p.seg_valid = true;
   return ok();
+}
+
+int pool_solve(Pool& p, const cgc_options* opts) {
+  if (int rc = pool_solve_async(p, opts)) return rc;
+  return pool_solve_wait(p);
 }
 
 int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host) {
   if (inst < 0 || inst >= p.ninst || !out || (which != CGC_SEG_SINK_REACH && which != CGC_SEG_SOURCE_MIN))
     return fail(CGC_ERR_ARG, "get_segments: bad arguments");
+  if (p.pending) return fail(CGC_ERR_STATE, "get_segments: wait for the solve first");
   if (!p.solved) return fail(CGC_ERR_STATE, "get_segments: call maxflow first");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
-  uint8_t* dst = host ? p.seg : out;
-  const unsigned blocks = (unsigned)std::min<int64_t>(std::max<int64_t>((N + 1023) / 1024, 1), 8 * (int64_t)p.sms);
-  k_segments_lin<<<blocks, 256, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
+  if ((host || !p.seg_valid || mask != 1 || bg != 0) && !p.segtmp) CGC_CUDA(cudaMalloc(&p.segtmp, p.maxN));
+  const unsigned blocks = (unsigned)std::min<int64_t>(std::max<int64_t>((N + 4095) / 4096, 1), 8 * (int64_t)p.sms);
+  const uint8_t* src = nullptr;  // device bytes to copy to `out` as they are
+  if (p.seg_valid) {
+    // the host-path solve wrote both sets as 1/0 bytes
+    const uint8_t* set = p.segbuf + (which == CGC_SEG_SOURCE_MIN ? 0 : p.sumN) + p.voff[inst];
+    if (mask == 1 && bg == 0) {
+      src = set;
+    } else {
+      uint8_t* dst = host ? p.segtmp : out;
+      k_mask_remap<<<blocks, 256, 0, p.stream>>>(set, dst, N, mask, bg); note_launch();
+      src = host ? p.segtmp : nullptr;
+    }
+  } else {
+    // after a device-resident solve: from the solver state
+    uint8_t* dst = host ? p.segtmp : out;
+    k_segments_lin<<<blocks, 256, 0, p.stream>>>(p.dp, inst, which, dst, mask, bg); note_launch();
+    src = host ? p.segtmp : nullptr;
+  }
   CGC_CUDA(cudaGetLastError());
-  if (host) CGC_CUDA(cudaMemcpyAsync(out, p.seg, N, cudaMemcpyDeviceToHost, p.stream));
+  if (src) CGC_CUDA(cudaMemcpyAsync(out, src, N, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p.stream));
   CGC_CUDA(cudaStreamSynchronize(p.stream));
   return ok();
 }
 
 int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess) {
   if (inst < 0 || inst >= p.ninst) return fail(CGC_ERR_ARG, "get_residuals: bad instance");
+  if (p.pending) return fail(CGC_ERR_STATE, "get_residuals: wait for the solve first");
   if (!p.solved) return fail(CGC_ERR_STATE, "get_residuals: call maxflow first");
   const InstGeo& G = p.geo[inst];
   const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  if (!p.resid) CGC_CUDA(cudaMalloc(&p.resid, (size_t)p.maxN * 4));
   const int blocks = (int)std::min<int64_t>((N + 255) / 256, 65535);
   auto one = [&](const int32_t* plane, int32_t* out) -> int {
     if (!out) return CGC_OK;
-    k_unpermute<<<blocks, 256, 0, p.stream>>>(p.dp, inst, plane, p.staging); note_launch();
+    k_unpermute<<<blocks, 256, 0, p.stream>>>(p.dp, inst, plane, p.resid); note_launch();
     CGC_CUDA(cudaGetLastError());
-    CGC_CUDA(cudaMemcpyAsync(out, p.staging, N * 4, cudaMemcpyDeviceToHost, p.stream));
+    CGC_CUDA(cudaMemcpyAsync(out, p.resid, N * 4, cudaMemcpyDeviceToHost, p.stream));
     CGC_CUDA(cudaStreamSynchronize(p.stream));
     return CGC_OK;
   };
@@ -1008,6 +1131,25 @@ int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int3
       if ((rc = one(p.dp.r + d * p.Np, res[d]))) return rc;
   if ((rc = one(p.dp.rT, resT))) return rc;
   if ((rc = one(p.dp.e, excess))) return rc;
+  return ok();
+}
+
+// Distance labels of the last solve in linear order (INT32_MIN where the
+// sink cannot be reached).
+int pool_labels(Pool& p, int inst, int32_t* labels) {
+  if (inst < 0 || inst >= p.ninst || !labels) return fail(CGC_ERR_ARG, "get_labels: bad arguments");
+  if (p.pending) return fail(CGC_ERR_STATE, "get_labels: wait for the solve first");
+  if (!p.solved) return fail(CGC_ERR_STATE, "get_labels: call maxflow first");
+  const InstGeo& G = p.geo[inst];
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  if (!p.resid) CGC_CUDA(cudaMalloc(&p.resid, (size_t)p.maxN * 4));
+  k_unpermute<<<(int)std::min<int64_t>((N + 255) / 256, 65535), 256, 0, p.stream>>>(p.dp, inst, p.dp.h, p.resid);
+  note_launch();
+  CGC_CUDA(cudaGetLastError());
+  CGC_CUDA(cudaMemcpyAsync(labels, p.resid, N * 4, cudaMemcpyDeviceToHost, p.stream));
+  CGC_CUDA(cudaStreamSynchronize(p.stream));
+  for (int64_t v = 0; v < N; ++v)
+    if (labels[v] >= INF) labels[v] = INT32_MIN;
   return ok();
 }
 
@@ -1087,6 +1229,17 @@ int cgc_grid_maxflow(cgc_grid* g, const cgc_options* opts, int64_t* flow) {
   if (flow) *flow = g->p->flows[0];
   return cgc::ok();
 }
+int cgc_grid_maxflow_async(cgc_grid* g, const cgc_options* opts) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_solve_async(*g->p, opts);
+}
+int cgc_grid_wait(cgc_grid* g, int64_t* flow) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  int rc = cgc::pool_solve_wait(*g->p);
+  if (rc) return rc;
+  if (flow) *flow = g->p->flows[0];
+  return cgc::ok();
+}
 int cgc_grid_get_segments(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background) {
   if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
   return cgc::pool_segments(*g->p, 0, which, out, mask, background, true);
@@ -1094,6 +1247,10 @@ int cgc_grid_get_segments(cgc_grid* g, int which, uint8_t* out, uint8_t mask, ui
 int cgc_grid_get_segments_device(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background) {
   if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
   return cgc::pool_segments(*g->p, 0, which, out, mask, background, false);
+}
+int cgc_grid_get_labels(cgc_grid* g, int32_t* labels) {
+  if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");
+  return cgc::pool_labels(*g->p, 0, labels);
 }
 int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, int32_t* excess) {
   if (!g) return cgc::fail(CGC_ERR_ARG, "null grid");

@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -35,15 +36,28 @@ struct Pool {
   int64_t Np = 0;
   DevPool dp{};
   void* dbuf = nullptr;          // all device state
-  int32_t* staging = nullptr;    // 2*maxN int32
-  // host uploads alternate between staging and staging2 on copy_stream
-  // (stage_upload in cgc_engine.cu); created on the first host upload
-  int32_t* staging2 = nullptr;   // 2*maxN int32
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t staged[2] = {nullptr, nullptr};    // the copy into buffer k has finished
-  cudaEvent_t consumed[2] = {nullptr, nullptr};  // the kernel reading buffer k has finished
-  int stage = 0;
-  uint8_t* seg = nullptr;        // maxN bytes
+  // Inputs of the set_* calls: linear (x-fastest) planes, the instances back
+  // to back at voff[i]; read by the fused upload kernel of the next solve.
+  int64_t sumN = 0;
+  std::vector<int64_t> voff;
+  int32_t* lin = nullptr;        // 5 planes of sumN: capS, capT, fwd x/y/z (first set_* call)
+  int32_t* lin_bwd = nullptr;    // 3 planes of sumN: bwd x/y/z (first asymmetric n-link upload)
+  std::vector<const int32_t*> host_in;  // 8 per instance: planes the next solve reads (null = zero)
+  const int32_t** d_host_in = nullptr;  // device copy of host_in (batches of more than one instance)
+  cudaStream_t copy_stream = nullptr;   // host -> device copies of the setters
+  cudaEvent_t inputs_read = nullptr;    // recorded after the upload kernel of the last solve
+  // cut sets of the last host-path solve (1/0 bytes, linear order): source
+  // side at [0, sumN), sink side at [sumN, 2 sumN)
+  uint8_t* segbuf = nullptr;
+  uint8_t** d_segtab = nullptr;  // 2 per instance: pointers into segbuf
+  bool seg_valid = false;        // segbuf holds the last solve's cut sets
+  uint8_t* segtmp = nullptr;     // maxN bytes for remapped masks (mask / background values)
+  int32_t* resid = nullptr;      // maxN int32 for cgc_grid_get_residuals
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // solve and kernel timing
+  bool pending = false;          // a host-path solve was enqueued and not yet waited for
+  int pending_persistent = 1;    // its options' persistent field
+  long long launches0 = 0;       // launch counter when it was enqueued
+  int64_t host_counts[3] = {0, 0, 0};  // host-driven schedule: sweeps, relabels, BFS rounds
   int32_t* pinned_cnt = nullptr; // host-pinned counters
   bool solved = false;
   int sms = 148;
@@ -77,14 +91,17 @@ struct Pool {
     if (d_in) cudaFree(d_in);
     if (d_out) cudaFree(d_out);
     if (dbuf) cudaFree(dbuf);
-    if (staging) cudaFree(staging);
-    if (staging2) cudaFree(staging2);
-    for (int k = 0; k < 2; ++k) {
-      if (staged[k]) cudaEventDestroy(staged[k]);
-      if (consumed[k]) cudaEventDestroy(consumed[k]);
-    }
+    if (lin) cudaFree(lin);
+    if (lin_bwd) cudaFree(lin_bwd);
+    if (d_host_in) cudaFree(d_host_in);
+    if (segbuf) cudaFree(segbuf);
+    if (d_segtab) cudaFree(d_segtab);
+    if (segtmp) cudaFree(segtmp);
+    if (resid) cudaFree(resid);
+    if (inputs_read) cudaEventDestroy(inputs_read);
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
     if (copy_stream) cudaStreamDestroy(copy_stream);
-    if (seg) cudaFree(seg);
     if (pinned_cnt) cudaFreeHost(pinned_cnt);
   }
 };
@@ -98,11 +115,19 @@ cgc_options resolve_options(const cgc_options* o);
 uint64_t wait_limit_ns(const cgc_options& o);
 SolveParams solve_params(const cgc_options& o);
 int pool_solve(Pool& p, const cgc_options* opts);
+// host path in two halves: enqueue a solve of the set_* inputs on p.stream
+// (no host synchronisation), then wait for it and read flows and statistics
+int pool_solve_async(Pool& p, const cgc_options* opts);
+int pool_solve_wait(Pool& p);
+// runs `launch` (a cooperative launch into `stream`) after every earlier
+// cooperative launch of this library on the device has ended
+int coop_launch_ordered(int device, cudaStream_t stream, const std::function<int()>& launch);
 // cooperative launch of the persistent solve kernel selected by the options
 int launch_solve(Pool& p, const cgc_options& o, const DevPool& d, const SolveParams& prm, cudaStream_t stream);
 int pool_segments(Pool& p, int inst, int which, uint8_t* out, uint8_t mask, uint8_t bg, bool host);
 int pool_residuals(Pool& p, int inst, int32_t* const res[6], int32_t* resT, int32_t* excess);
 int pool_trace(Pool& p, int64_t* out, int32_t cap, int32_t* count);
+int pool_labels(Pool& p, int inst, int32_t* labels);
 // device-resident batch path (cgc_batch.cu)
 int pool_bind_inputs(Pool& p, int inst, const int32_t* capS, const int32_t* capT, const int32_t* const fwd[3],
                      const int32_t* const bwd[3]);

@@ -175,6 +175,20 @@ class GridGraph:
         self.flow = int(flow.value)
         return self.flow
 
+    def max_flow_async(self, policy: Policy | None = None) -> None:
+        """Queues the solve of the capacities set so far on the grid's stream and
+        returns at once; wait() blocks until it is done and returns the flow.
+        Meanwhile another grid's set_* calls can copy its inputs to the device,
+        so uploads and solves of consecutive grids overlap."""
+        opts = policy.options() if policy else None
+        check(self._lib.cgc_grid_maxflow_async(self._h, C.byref(opts) if opts else None))
+
+    def wait(self) -> int:
+        flow = C.c_int64()
+        check(self._lib.cgc_grid_wait(self._h, C.byref(flow)))
+        self.flow = int(flow.value)
+        return self.flow
+
     def fill_segments(self, out: np.ndarray | None = None, mask: int = 255, background: int = 0,
                       which: str = SINK) -> np.ndarray:
         """out[v] = mask where v is in the chosen set, else background.
@@ -199,6 +213,13 @@ class GridGraph:
         ptrs = (C.c_void_p * 6)(*[r[d].ctypes.data for d in range(6)])
         check(self._lib.cgc_grid_get_residuals(self._h, ptrs, _ptr(rt), _ptr(ex)))
         return {"r": r, "resT": rt, "excess": ex}
+
+    def labels(self) -> np.ndarray:
+        """Distance to the sink after the final global relabel, per voxel (linear
+        layout); INT32_MIN where the sink cannot be reached."""
+        out = np.empty(self.n, dtype=np.int32)
+        check(self._lib.cgc_grid_get_labels(self._h, _ptr(out)))
+        return out
 
     def stats(self) -> dict:
         s = _lib.Stats()
@@ -229,7 +250,7 @@ class GridGraph:
         return _autotune(self._lib.cgc_grid_autotune, self._h, candidates, repeats)
 
 
-TRACE_KINDS = {1: "bfs_round", 2: "relabel_done", 3: "sweep", 4: "reach_round"}
+TRACE_KINDS = {1: "bfs_round", 2: "relabel_done", 3: "sweep", 4: "reach_round", 5: "flow"}
 
 
 def _read_trace(fn, handle) -> list:
@@ -240,8 +261,9 @@ def _read_trace(fn, handle) -> list:
     out = []
     for i in range(n.value):
         w = int(buf[2 * i]) & 0xFFFFFFFFFFFFFFFF
-        out.append({"kind": TRACE_KINDS.get(w >> 56, w >> 56), "index": (w >> 24) & 0xFFFFFFFF,
-                    "tiles": w & 0xFFFFFF, "ns": int(buf[2 * i + 1])})
+        rec = {"kind": TRACE_KINDS.get(w >> 56, w >> 56), "index": (w >> 24) & 0xFFFFFFFF, "tiles": w & 0xFFFFFF}
+        rec["flow" if (w >> 56) == 5 else "ns"] = int(buf[2 * i + 1])
+        out.append(rec)
     return out
 
 

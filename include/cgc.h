@@ -90,7 +90,7 @@ typedef struct cgc_stats {
   int64_t tiles_swept;       /* tile visits by the push sweep */
   int64_t tiles_relabelled;  /* tile visits by the BFS */
   int64_t pulses;            /* total local pulses executed over all tile visits */
-  double  solve_ms;          /* device time of the last maxflow (preparation + solve) */
+  double  solve_ms;          /* device time of the last maxflow (upload, preflow, solve and both cut sets) */
   double  kernel_ms;         /* device time of the solve kernel(s) alone */
   int64_t launches;          /* kernels launched by the last maxflow */
   double  bfs_ms;            /* persistent solve: time in exact global relabels */
@@ -160,6 +160,9 @@ int cgc_graph_set_tlinks(cgc_graph* g, const int32_t* capS, const int32_t* capT)
 int cgc_graph_maxflow(cgc_graph* g, const cgc_options* opts, int64_t* flow);
 int cgc_graph_get_segments(cgc_graph* g, int which, uint8_t* out, uint8_t mask, uint8_t background);
 int cgc_graph_stats(cgc_graph* g, cgc_stats* stats);
+/* Final distance labels (INT32_MIN where the sink cannot be reached) and
+ * excess per vertex of the last solve (host arrays of n, either may be NULL). */
+int cgc_graph_get_state(cgc_graph* g, int32_t* labels, int32_t* excess);
 
 /* Same as the two setters above with device pointers (no host copies). */
 int cgc_grid_set_tlinks_device(cgc_grid* g, const int32_t* capS, const int32_t* capT);
@@ -173,6 +176,20 @@ int cgc_grid_set_nlinks_device(cgc_grid* g, int axis, const int32_t* fwd, const 
  * after new set_* calls. */
 int cgc_grid_maxflow(cgc_grid* g, const cgc_options* opts, int64_t* flow);
 
+/* The same solve in two halves, for callers that overlap the host uploads of
+ * one grid with the solve of another (no counterpart in the reference, whose
+ * max_flow blocks, graph_cut.hpp:69-100).  cgc_grid_maxflow_async queues the
+ * solve of the capacities set so far (fused upload and preflow, the solve and
+ * both cut sets) on the grid's stream and returns without waiting; errors
+ * found on the device are reported by cgc_grid_wait, which blocks until the
+ * solve is done and writes the flow (may be NULL).  Between the two calls the
+ * grid's set_* calls may already copy the next inputs (they wait until the
+ * queued solve has read the previous ones), while the calls that read results
+ * or solve (maxflow, get_segments, get_residuals, autotune) return
+ * CGC_ERR_STATE.  To overlap two grids, give each its own stream. */
+int cgc_grid_maxflow_async(cgc_grid* g, const cgc_options* opts);
+int cgc_grid_wait(cgc_grid* g, int64_t* flow);
+
 /* Replaces Graph::fill_segments (graph_cut.hpp:318-333): out[v] = mask if v is
  * in the chosen set (CGC_SEG_*), else background.  Host array of X*Y*Z. */
 int cgc_grid_get_segments(cgc_grid* g, int which, uint8_t* out, uint8_t mask, uint8_t background);
@@ -185,14 +202,21 @@ int cgc_grid_get_segments_device(cgc_grid* g, int which, uint8_t* out, uint8_t m
  * certificates and tests; any pointer may be NULL. */
 int cgc_grid_get_residuals(cgc_grid* g, int32_t* const res[6], int32_t* resT, int32_t* excess);
 
+/* Distance labels of the last solve (host array of X*Y*Z, linear layout): the
+ * exact distance to the sink found by the final global relabel, INT32_MIN
+ * (the reference's INVALID_LABEL, detail/graph_cut_policies.hpp:34) where the
+ * sink cannot be reached.  For trace objects and tests. */
+int cgc_grid_get_labels(cgc_grid* g, int32_t* labels);
+
 int cgc_grid_stats(cgc_grid* g, cgc_stats* out);
 
 /* Phase trace of the last persistent solve (extends the reference's trace
  * hooks, graph_cut.hpp:26-45, with per-step detail): *count receives the
  * number of records; up to `cap` records of two int64 each are copied to out:
  * word 0 = kind << 56 | index << 24 | tiles (kind 1 = BFS round, 2 = global
- * relabel done (tiles = active tiles), 3 = sweep, 4 = reachability round),
- * word 1 = nanoseconds since the launch. */
+ * relabel done (tiles = active tiles), 3 = sweep, 4 = reachability round,
+ * 5 = flow at global relabel `index`), word 1 = nanoseconds since the launch
+ * (kind 5: the exact flow delivered so far). */
 int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count);
 
 /* ---- allocation-free solve of a small grid ---------------------------------
@@ -214,7 +238,8 @@ int cgc_grid_trace(cgc_grid* g, int64_t* out, int32_t cap, int32_t* count);
  * supported.  Every call blocks the calling thread: it waits for `stream` and
  * reads the flow and the device status back into host memory before it
  * returns.  Calls share the array: calls that overlap on the GPU race and must
- * not be issued. */
+ * not be issued, and a call should not overlap another solve of this library
+ * on another stream (both are grid-wide cooperative launches). */
 #define CGC_NOALLOC_MAX_VOXELS 262144
 int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const int32_t* capS, const int32_t* capT,
                              const int32_t* const fwd[3], const int32_t* const bwd[3],

@@ -95,17 +95,77 @@ struct GraphCutPolicy {
   }
 };
 
-// Trace protocol of the reference.  The solve runs as one device launch, so
-// the per-iteration hooks are replayed after it: one iteration per exact
-// global relabel, with the level starts of that relabel's BFS rounds from the
-// solve's phase trace.
+class GridGraph;
+class GenericGraph;
+template <typename TFlow>
+class Graph;
+
+// Read-only view of a solve handed to the trace hooks, in place of the
+// reference's device-side GraphCutData (detail/graph_cut_data.hpp:20-140,
+// passed by MinCut::compute, detail/graph_cut_implementation.hpp:134-196):
+//  * vertexCount() and mEdgeCount as there;
+//  * iteration() (-1 before the first) and flow(): the exact flow delivered
+//    when the reported iteration's push phase ended (0 in computationStarted;
+//    -1 where the engine keeps no per-iteration record: generic graphs);
+//  * for the final state (finalState(): the last afterPush and
+//    computationFinished), host copies in vertex-id order, read from the device
+//    on first use: vertexExcess() and labels() (the distance to the sink after
+//    the last exact relabel, INVALID_LABEL where the sink cannot be reached --
+//    the reference's label convention, graph_cut_policies.hpp:34).  Earlier
+//    states are not kept: the whole solve is one device launch.
+// Without the reference's CSR layout there are no device arrays to hand out.
+template <typename TFlow>
+class GraphCutData {
+ public:
+  static const int INVALID_LABEL = INT32_MIN;
+  int mEdgeCount = 0;
+
+  int vertexCount() const { return n_; }
+  int iteration() const { return iteration_; }
+  int64_t flow() const { return flow_; }
+  bool finalState() const { return final_; }
+  const cgc_stats& stats() const { return stats_; }
+  const std::vector<TFlow>& vertexExcess() const {
+    load();
+    return excess_;
+  }
+  const std::vector<int>& labels() const {
+    load();
+    return labels_;
+  }
+
+ private:
+  template <typename T>
+  friend class Graph;
+  void load() const;
+
+  int n_ = 0;
+  int iteration_ = -1;
+  int64_t flow_ = 0;
+  bool final_ = false;
+  cgc_stats stats_{};
+  const GridGraph* grid_ = nullptr;
+  const GenericGraph* generic_ = nullptr;
+  mutable bool loaded_ = false;
+  mutable std::vector<TFlow> excess_;
+  mutable std::vector<int> labels_;
+};
+
+// Trace protocol of the reference (graph_cut.hpp:26-45).  The solve runs as
+// one device launch, so the per-iteration hooks are replayed after it: one
+// iteration per exact global relabel, with the level starts of that relabel's
+// BFS rounds and the flow at the end of its push phase from the solve's phase
+// trace.  afterRelabel's level starts also bind to a parameter of type
+// const thrust::host_vector<int>& (thrust converts from std::vector).
 struct DummyTraceObject {
-  void computationStarted(const cgc_stats&) {}
+  template <typename TFlow>
+  void computationStarted(const GraphCutData<TFlow>&) {}
   void beginIteration(int) {}
   void afterRelabel(int, const std::vector<int>&) {}
-  void afterPush(int, bool, const cgc_stats&) {}
   template <typename TFlow>
-  void computationFinished(TFlow, const cgc_stats&) {}
+  void afterPush(int, bool, const GraphCutData<TFlow>&) {}
+  template <typename TFlow>
+  void computationFinished(TFlow, const GraphCutData<TFlow>&) {}
 };
 
 namespace detail {
@@ -148,6 +208,9 @@ class GridGraph {
   void segments(int which, uint8_t* out, uint8_t mask = 255, uint8_t bg = 0) const {
     check(cgc_grid_get_segments(g_, which, out, mask, bg), "fill_segments");
   }
+  // distance labels (INT32_MIN: cannot reach the sink) and excess of the last solve
+  void labels(int32_t* out) const { check(cgc_grid_get_labels(g_, out), "labels"); }
+  void excess(int32_t* out) const { check(cgc_grid_get_residuals(g_, nullptr, nullptr, out), "excess"); }
   cgc_stats stats() const {
     cgc_stats s;
     check(cgc_grid_stats(g_, &s), "stats");
@@ -155,12 +218,13 @@ class GridGraph {
   }
   // Phase records of the last persistent solve (cgc_grid_trace): kind 1 = BFS
   // round, 2 = global relabel done (tiles = active tiles), 3 = sweep, 4 =
-  // reachability round; `tiles` = tiles in the round; `ns` since the launch.
+  // reachability round, 5 = flow at a global relabel; `tiles` = tiles in the
+  // round; `value` = ns since the launch (kind 5: the exact flow so far).
   struct PhaseRecord {
     int kind;
     int64_t index;
     int tiles;
-    int64_t ns;
+    int64_t value;
   };
   std::vector<PhaseRecord> trace() const {
     int32_t n = 0;
@@ -205,6 +269,8 @@ class GenericGraph {
   void segments(int which, uint8_t* out, uint8_t mask = 255, uint8_t bg = 0) const {
     check(cgc_graph_get_segments(g_, which, out, mask, bg), "fill_segments");
   }
+  // distance labels (INT32_MIN: cannot reach the sink) and excess of the last solve
+  void state(int32_t* labels, int32_t* excess) const { check(cgc_graph_get_state(g_, labels, excess), "state"); }
   cgc_stats stats() const {
     cgc_stats s;
     check(cgc_graph_stats(g_, &s), "stats");
@@ -215,6 +281,21 @@ class GenericGraph {
   cgc_graph* g_ = nullptr;
   int32_t n_;
 };
+
+template <typename TFlow>
+void GraphCutData<TFlow>::load() const {
+  if (loaded_ || !final_) return;  // earlier states are not kept
+  loaded_ = true;
+  std::vector<int32_t> ex((size_t)n_), lb((size_t)n_);
+  if (grid_) {
+    grid_->excess(ex.data());
+    grid_->labels(lb.data());
+  } else if (generic_) {
+    generic_->state(lb.data(), ex.data());
+  }
+  excess_.assign(ex.begin(), ex.end());
+  labels_.assign(lb.begin(), lb.end());
+}
 
 // Drop-in for cugip::Graph<TFlow> (graph_cut.hpp:47-146).  An edge list that
 // forms a 6-connected grid with linear vertex ids goes to the tile engine,
@@ -243,6 +324,7 @@ class Graph {
     int32_t dims[3];
     grid_.reset();
     generic_.reset();
+    edges_ = edge_count;
     const int rc = cgc_grid_create_from_edges(n_, edge_count, a.data(), b.data(), f.data(), w.data(), nullptr, &g, dims);
     if (rc == CGC_ERR_NOT_GRID) {
       std::vector<int32_t> ai(a.begin(), a.end()), bi(b.begin(), b.end());
@@ -266,6 +348,18 @@ class Graph {
     DummyTraceObject trace;
     return max_flow_with_tracing(trace);
   }
+  // The flow as an exact int64.  max_flow() returns it converted to TFlow,
+  // which for Graph<float> rounds flows above 2^24 (float's 24-bit mantissa).
+  int64_t max_flow_exact() {
+    max_flow();
+    return last_flow_;
+  }
+  template <typename TPolicy>
+  int64_t max_flow_exact(TPolicy& policy) {
+    max_flow(policy);
+    return last_flow_;
+  }
+  int64_t last_flow() const { return last_flow_; }
   template <typename TPolicy>
   TFlow max_flow(TPolicy& policy) {
     DummyTraceObject trace;
@@ -279,17 +373,24 @@ class Graph {
   template <typename TPolicy, typename TTraceObject>
   TFlow max_flow_with_tracing(TPolicy& policy, TTraceObject& trace) {
     if (!grid_ && !generic_) throw Exception(CGC_ERR_STATE, "max_flow: set_nweights was not called");
-    cgc_stats before{};
-    trace.computationStarted(before);
+    GraphCutData<TFlow> data;
+    data.n_ = n_;
+    data.mEdgeCount = edges_;
+    data.grid_ = grid_.get();
+    data.generic_ = generic_.get();
+    trace.computationStarted(data);
     const GraphCutPolicy& p = policy;
     const int64_t f = grid_ ? grid_->max_flow(&p) : generic_->max_flow(&p);
-    const cgc_stats st = grid_ ? grid_->stats() : generic_->stats();
+    last_flow_ = f;
+    data.stats_ = grid_ ? grid_->stats() : generic_->stats();
     // One iteration per exact global relabel, as in the reference's MinCut
     // loop (detail/graph_cut_implementation.hpp:150-175).  afterRelabel gets
     // the level starts of that relabel's BFS: the running count of tiles
     // visited per BFS round (the reference counts vertices per level); the
-    // push phase that follows is reported by afterPush.
+    // push phase that follows is reported by afterPush, with the flow at the
+    // next relabel (the final flow after the last iteration).
     std::vector<std::vector<int>> levels;
+    std::vector<int64_t> flow_at;  // flow_at[r]: flow at global relabel r + 1
     if (grid_) {
       std::vector<int> cur{0};
       for (const auto& r : grid_->trace()) {
@@ -298,16 +399,25 @@ class Graph {
         } else if (r.kind == 2) {
           levels.push_back(cur);
           cur.assign(1, 0);
+        } else if (r.kind == 5) {
+          flow_at.push_back(r.value);
         }
       }
     }
-    const int64_t iters = st.global_relabels;
+    const int64_t iters = data.stats_.global_relabels;
     for (int64_t i = 0; i < iters; ++i) {
+      const bool last = i + 1 == iters;
+      data.iteration_ = (int)i;
+      data.final_ = last;
+      data.flow_ = last ? f : (i + 1 < (int64_t)flow_at.size() ? flow_at[(size_t)i + 1] : -1);
       trace.beginIteration((int)i);
       trace.afterRelabel((int)i, i < (int64_t)levels.size() ? levels[(size_t)i] : std::vector<int>{0});
-      trace.afterPush((int)i, i + 1 == iters, st);
+      trace.afterPush((int)i, last, data);
     }
-    trace.computationFinished(static_cast<TFlow>(f), st);
+    data.final_ = true;
+    data.flow_ = f;
+    const GraphCutData<TFlow>& done = data;
+    trace.computationFinished(static_cast<TFlow>(f), done);
     return static_cast<TFlow>(f);
   }
 
@@ -353,6 +463,8 @@ class Graph {
   };
 
   int n_ = 0;
+  int edges_ = 0;
+  int64_t last_flow_ = 0;
   Owned<GridGraph> grid_;
   Owned<GenericGraph> generic_;
   std::vector<int32_t> tlink_s_, tlink_t_;  // host copy of the last t-links

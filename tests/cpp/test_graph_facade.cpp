@@ -6,8 +6,10 @@
 // cgc::GridGraph.
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
+#include <cgc/cugip.hpp>
 #include <cgc/graph_cut.hpp>
 
 #define EXPECT(c)                                                       \
@@ -25,10 +27,85 @@ struct CountingTrace : cgc::DummyTraceObject {
     for (size_t i = 1; i < starts.size(); ++i) levels_ok = levels_ok && starts[i] >= starts[i - 1];
     last_levels = (int)starts.size();
   }
-  void afterPush(int, bool done, const cgc_stats&) { ++pushes; done_seen = done_seen || done; }
   template <typename T>
-  void computationFinished(T flow, const cgc_stats&) { finished = (long long)flow; }
+  void afterPush(int, bool done, const cgc::GraphCutData<T>&) { ++pushes; done_seen = done_seen || done; }
+  template <typename T>
+  void computationFinished(T flow, const cgc::GraphCutData<T>&) { finished = (long long)flow; }
 };
+
+// A trace object with the hook signatures of the reference benchmark's
+// TraceObject (benchmarks/graph_cut/graph_cut.cu:82-177): non-const
+// GraphCutData<float>& in computationStarted / afterPush, a const one in
+// computationFinished, which checks the reference's invariant (excess only at
+// vertices whose label is invalid, graph_cut.cu:171).
+struct ReferenceShapedTrace {
+  int vertices = 0, edges = 0, iterations = 0;
+  size_t level_entries = 0;
+  std::vector<long long> flows;
+  bool done = false, invariant = false;
+  float final_flow = -1.f;
+  void computationStarted(cugip::GraphCutData<float>& aData) {
+    vertices = aData.vertexCount();
+    edges = aData.mEdgeCount;
+  }
+  void beginIteration(int) { ++iterations; }
+  void afterRelabel(int, const std::vector<int>& aLevelStarts) { level_entries += aLevelStarts.size(); }
+  void afterPush(int, bool aDone, cugip::GraphCutData<float>& aGraph) {
+    flows.push_back((long long)aGraph.flow());
+    done = aDone;
+  }
+  void computationFinished(float aFlow, const cugip::GraphCutData<float>& aData) {
+    final_flow = aFlow;
+    const std::vector<float>& excess = aData.vertexExcess();
+    const std::vector<int>& labels = aData.labels();
+    invariant = (int)excess.size() == aData.vertexCount() && labels.size() == excess.size();
+    for (size_t i = 0; i < excess.size() && invariant; ++i)
+      invariant = excess[i] <= 0.0f || labels[i] == cugip::GraphCutData<float>::INVALID_LABEL;
+  }
+};
+
+// The 512x512x128 tube workload (flow 22 895 482, above float's 2^24) given
+// to cugip::Graph<float> as an edge list, as the reference's front-end builds
+// it: the exact flow through max_flow_exact and the trace protocol.
+void full_size_tubes() {
+  cgc_volume_spec spec;
+  EXPECT(cgc_volume_preset(3, 0, &spec) == CGC_OK);
+  const int64_t X = spec.X, Y = spec.Y, Z = spec.Z, N = X * Y * Z;
+  std::vector<int32_t> cs(N), ct(N), nx(N), ny(N), nz(N);
+  EXPECT(cgc_volume_generate(&spec, cs.data(), ct.data(), nx.data(), ny.data(), nz.data(), nullptr) == CGC_OK);
+  std::vector<cugip::EdgeRecord> edges;
+  std::vector<float> w;
+  edges.reserve(3 * N);
+  w.reserve(3 * N);
+  for (int64_t z = 0; z < Z; ++z)
+    for (int64_t y = 0; y < Y; ++y)
+      for (int64_t x = 0; x < X; ++x) {
+        const int64_t v = x + X * (y + Y * z);
+        if (x + 1 < X) { edges.emplace_back((unsigned)v, (unsigned)(v + 1)); w.push_back((float)nx[v]); }
+        if (y + 1 < Y) { edges.emplace_back((unsigned)v, (unsigned)(v + X)); w.push_back((float)ny[v]); }
+        if (z + 1 < Z) { edges.emplace_back((unsigned)v, (unsigned)(v + X * Y)); w.push_back((float)nz[v]); }
+      }
+  std::vector<float> s(cs.begin(), cs.end()), t(ct.begin(), ct.end());
+  cugip::Graph<float> graph;
+  graph.set_vertex_count((int)N);
+  graph.set_nweights((int)edges.size(), edges.data(), w.data(), w.data());
+  graph.set_tweights(s.data(), t.data());
+  EXPECT(graph.grid() != nullptr);
+  ReferenceShapedTrace trace;
+  const float f = graph.max_flow_with_tracing(trace);
+  EXPECT(graph.last_flow() == 22895482LL);
+  EXPECT((double)f == (double)(float)22895482LL);
+  EXPECT(trace.vertices == (int)N && trace.edges == (int)edges.size());
+  EXPECT(trace.iterations >= 1 && (int)trace.flows.size() == trace.iterations && trace.done);
+  for (size_t i = 1; i < trace.flows.size(); ++i) EXPECT(trace.flows[i] >= trace.flows[i - 1]);
+  EXPECT(trace.flows.back() == 22895482LL);
+  EXPECT(trace.invariant && trace.level_entries >= (size_t)trace.iterations);
+  // a second solve with new weights through the exact accessor
+  graph.set_tweights(s.data(), t.data());
+  graph.set_nweights((int)edges.size(), edges.data(), w.data(), w.data());
+  EXPECT(graph.max_flow_exact() == 22895482LL);
+  std::printf("full size ok\n");
+}
 
 template <typename W>
 void four_by_four() {
@@ -96,7 +173,11 @@ void layered(bool flip, long long expected) {
   EXPECT(seg[sink_first] == 255 && seg[flip ? (layers - 1) * size : 0] == 0);
 }
 
-int main() {
+int main(int argc, char** argv) {
+  if (argc > 1 && std::string(argv[1]) == "--full-size") {
+    full_size_tubes();
+    return 0;
+  }
   four_by_four<float>();
   four_by_four<int>();
   layered<float>(false, 1024 * 8);

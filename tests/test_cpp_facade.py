@@ -27,3 +27,14 @@ def test_facade_runs_reference_style_graph(tmp_path):
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "cpp facade ok" in out.stdout
+
+
+@pytest.mark.gpu
+def test_facade_exact_flow_and_reference_shaped_trace_on_512x512x128(tmp_path):
+    """cugip::Graph<float> (include/cgc/cugip.hpp) on the 512x512x128 tube
+    workload as an edge list: exact int64 flow and a trace object with the
+    reference benchmark's hook signatures."""
+    exe = compile_facade_test(tmp_path)
+    out = subprocess.run([exe, "--full-size"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "full size ok" in out.stdout
