@@ -49,16 +49,6 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
-class VolumeSpec(C.Structure):
-    _fields_ = [("X", C.c_int32), ("Y", C.c_int32), ("Z", C.c_int32), ("kind", C.c_int32),
-                ("seed", C.c_uint64), ("count", C.c_int32), ("n_fixed_radii", C.c_int32),
-                ("fixed_radii", C.c_double * 8), ("radius_min", C.c_double), ("radius_max", C.c_double),
-                ("intensity_min", C.c_double), ("intensity_max", C.c_double), ("background", C.c_double),
-                ("noise_sd", C.c_double), ("mu_bg", C.c_double), ("mu_fg", C.c_double), ("class_sd", C.c_double),
-                ("tlink_scale", C.c_double), ("nlink_scale", C.c_double), ("nlink_sigma", C.c_double),
-                ("ctrl_min", C.c_int32), ("ctrl_max", C.c_int32), ("edge_sigma", C.c_double)]
-
-
 P32 = C.POINTER(C.c_int32)
 PU32 = C.POINTER(C.c_uint32)
 PU8 = C.POINTER(C.c_uint8)
@@ -127,8 +117,6 @@ SIGNATURES = {
     "cgc_trainer_weights": (C.c_int, [VP, VP, VP]),
     "cgc_build_segmentation_graph": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, VP, VP, C.c_float, C.c_int32,
                                                C.c_int32, C.c_int32, VP, VP, VP, VP, VP, VP]),
-    "cgc_volume_preset": (C.c_int, [C.c_int, C.c_int32, C.POINTER(VolumeSpec)]),
-    "cgc_volume_generate": (C.c_int, [C.POINTER(VolumeSpec), VP, VP, VP, VP, VP, VP]),
 }
 
 _lib = None

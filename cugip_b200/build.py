@@ -14,9 +14,12 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcgc.so")
+# synthetic workloads: host code only, so that CPU-only callers need no CUDA library
+VOL_LIB = os.path.join(HERE, "libcgcvol.so")
+VOL_SOURCES = ["cgc_volume.cpp"]
 
 SOURCES = ["cgc_engine.cu", "cgc_batch.cu", "cgc_autotune.cu", "cgc_sched_train.cu", "cgc_noalloc.cu",
-           "cgc_build.cu", "cgc_csr.cu", "cgc_volume.cpp", "cgc_graph.cpp"]
+           "cgc_build.cu", "cgc_csr.cu", "cgc_graph.cpp"]
 HEADERS = ["cgc_device.cuh", "cgc_kernels.cuh", "cgc_internal.h", "cgc_pool.h", "cgc_sched.cuh",
            "cgc_sync.cuh", "cgc_warp.cuh"]
 
@@ -40,7 +43,22 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_volume(force: bool = False, verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, s) for s in VOL_SOURCES] + [os.path.join(INCLUDE, "cgc_volume.h"),
+                                                            os.path.join(INCLUDE, "cgc.h"), __file__]
+    if not force and not _stale(VOL_LIB, deps):
+        return VOL_LIB
+    cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-fopenmp", "-I", INCLUDE, "-o", VOL_LIB + ".tmp",
+           *[os.path.join(CSRC, s) for s in VOL_SOURCES]]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(VOL_LIB + ".tmp", VOL_LIB)
+    return VOL_LIB
+
+
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    build_volume(force, verbose)
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(INCLUDE, "cgc.h"), __file__]
     if not force and not _stale(LIB, deps):
         return LIB

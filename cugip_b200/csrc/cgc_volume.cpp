@@ -18,10 +18,18 @@
 #include <vector>
 #include <algorithm>
 
-#include "cgc.h"
-#include "cgc_internal.h"
+#include <string>
+
+#include "cgc_volume.h"
 
 namespace {
+
+thread_local std::string g_volume_error;
+
+int fail(int code, const char* msg) {
+  g_volume_error = msg;
+  return code;
+}
 
 struct Rng {
   std::mt19937_64 eng;
@@ -149,8 +157,10 @@ inline int32_t round_cap(double v) {
 
 }  // namespace
 
+extern "C" const char* cgc_volume_last_error(void) { return g_volume_error.c_str(); }
+
 extern "C" int cgc_volume_preset(int which, int32_t index, cgc_volume_spec* out) {
-  if (!out) return cgc::fail(CGC_ERR_ARG, "cgc_volume_preset: null output");
+  if (!out) return fail(CGC_ERR_ARG, "cgc_volume_preset: null output");
   cgc_volume_spec s;
   std::memset(&s, 0, sizeof(s));
   s.kind = 0;
@@ -173,7 +183,7 @@ extern "C" int cgc_volume_preset(int which, int32_t index, cgc_volume_spec* out)
       s.background = 0.3; s.mu_bg = 0.3; s.mu_fg = 0.7; s.noise_sd = 0.1; s.ctrl_min = 4; s.ctrl_max = 6;
       break;
     case 4: {  // batched instance: extents U[32,160], 4..20 spheres r in [4, min/4]
-      if (index < 0) return cgc::fail(CGC_ERR_ARG, "cgc_volume_preset: negative index");
+      if (index < 0) return fail(CGC_ERR_ARG, "cgc_volume_preset: negative index");
       s.seed = 1000 + uint64_t(index);
       Rng rng(s.seed ^ 0x9E3779B97F4A7C15ull);
       s.X = rng.uniform_int(32, 160); s.Y = rng.uniform_int(32, 160); s.Z = rng.uniform_int(32, 160);
@@ -183,12 +193,12 @@ extern "C" int cgc_volume_preset(int which, int32_t index, cgc_volume_spec* out)
       break;
     }
     case 5:  // 128^3 training instance with the 64^3 generator's objects
-      if (index < 0) return cgc::fail(CGC_ERR_ARG, "cgc_volume_preset: negative index");
+      if (index < 0) return fail(CGC_ERR_ARG, "cgc_volume_preset: negative index");
       s.X = s.Y = s.Z = 128; s.seed = 10000 + uint64_t(index); s.count = 2; s.n_fixed_radii = 2;
       s.fixed_radii[0] = 12; s.fixed_radii[1] = 16; s.noise_sd = 0.05;
       break;
     default:
-      return cgc::fail(CGC_ERR_ARG, "cgc_volume_preset: unknown workload");
+      return fail(CGC_ERR_ARG, "cgc_volume_preset: unknown workload");
   }
   *out = s;
   return CGC_OK;
@@ -196,13 +206,13 @@ extern "C" int cgc_volume_preset(int which, int32_t index, cgc_volume_spec* out)
 
 extern "C" int cgc_volume_generate(const cgc_volume_spec* spec, int32_t* capS, int32_t* capT, int32_t* nx,
                                    int32_t* ny, int32_t* nz, float* image) {
-  if (!spec || !capS || !capT || !nx || !ny || !nz) return cgc::fail(CGC_ERR_ARG, "cgc_volume_generate: null pointer");
+  if (!spec || !capS || !capT || !nx || !ny || !nz) return fail(CGC_ERR_ARG, "cgc_volume_generate: null pointer");
   const cgc_volume_spec& s = *spec;
-  if (s.X <= 0 || s.Y <= 0 || s.Z <= 0) return cgc::fail(CGC_ERR_ARG, "cgc_volume_generate: bad extent");
-  if (s.kind == 1 && (s.ctrl_min < 2 || s.ctrl_max < s.ctrl_min)) return cgc::fail(CGC_ERR_ARG, "cgc_volume_generate: bad control point range");
+  if (s.X <= 0 || s.Y <= 0 || s.Z <= 0) return fail(CGC_ERR_ARG, "cgc_volume_generate: bad extent");
+  if (s.kind == 1 && (s.ctrl_min < 2 || s.ctrl_max < s.ctrl_min)) return fail(CGC_ERR_ARG, "cgc_volume_generate: bad control point range");
   const int64_t X = s.X, Y = s.Y, Z = s.Z, N = X * Y * Z;
   std::vector<float> img;
-  try { img.assign(size_t(N), float(s.background)); } catch (...) { return cgc::fail(CGC_ERR_OOM, "cgc_volume_generate: host allocation"); }
+  try { img.assign(size_t(N), float(s.background)); } catch (...) { return fail(CGC_ERR_OOM, "cgc_volume_generate: host allocation"); }
   Rng rng(s.seed);
   if (s.kind == 0) draw_spheres(img, s, rng); else draw_tubes(img, s, rng);
   // noise (one sequential stream, so the volume does not depend on the thread

@@ -11,6 +11,7 @@
 
 #include <cgc/cugip.hpp>
 #include <cgc/graph_cut.hpp>
+#include <cgc_volume.h>
 
 #define EXPECT(c)                                                       \
   do {                                                                  \

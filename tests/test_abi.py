@@ -29,6 +29,24 @@ def test_library_exports_every_declared_symbol():
         assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
 
 
+def test_volume_library_is_host_only_and_exports_its_header():
+    """libcgcvol.so (the synthetic workloads) exports every function of
+    include/cgc_volume.h and links no CUDA library, so the CPU baseline can
+    build workloads without the GPU engine."""
+    from cugip_b200 import volume
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "cgc_volume.h")).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(cgc_[a-z0-9_]+)\s*\(", text)))
+    lib = volume.load()
+    assert names == ["cgc_volume_generate", "cgc_volume_last_error", "cgc_volume_preset"]
+    for name in names:
+        assert hasattr(lib, name), name
+    import subprocess
+    deps = subprocess.run(["ldd", volume.VOL_LIB_PATH], capture_output=True, text=True).stdout
+    assert "libcuda" not in deps and "libcudart" not in deps, deps
+    with pytest.raises(_lib.CgcError):
+        volume.preset(99)
+
+
 def test_no_device_is_reported_not_hidden():
     import torch
     if torch.cuda.is_available():

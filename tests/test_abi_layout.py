@@ -15,18 +15,19 @@ import subprocess
 
 import pytest
 
-from cugip_b200 import _lib
+from cugip_b200 import _lib, volume
 from cugip_b200.graph_cut import Policy
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(ROOT, "cugip_b200")
 
-MIRRORS = [("cgc_options", _lib.Options), ("cgc_stats", _lib.Stats), ("cgc_volume_spec", _lib.VolumeSpec)]
+MIRRORS = [("cgc_options", _lib.Options), ("cgc_stats", _lib.Stats), ("cgc_volume_spec", volume.VolumeSpec)]
 
 
 def _c_layout(tmp_path) -> dict:
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cgc.h"', "int main(void) {"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cgc.h"', '#include "cgc_volume.h"',
+             "int main(void) {"]
     for cname, py in MIRRORS:
         lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
         for field, _ in py._fields_:

@@ -13,7 +13,7 @@ LIBDIR = os.path.join(ROOT, "cugip_b200")
 def compile_facade_test(tmp_path) -> str:
     exe = str(tmp_path / "test_graph_facade")
     subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
-                    SRC, "-L", LIBDIR, "-lcgc", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+                    SRC, "-L", LIBDIR, "-lcgc", "-lcgcvol", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
     return exe
 
 
