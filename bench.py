@@ -167,6 +167,87 @@ def profiled_traffic(workload: int):
     return None
 
 
+BATCH_CANDIDATES = [dict(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, bfs_warp_min=bw)
+                    for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8))
+                    for c in (2, 3, 4) for bw in ((0, 8) if c > 2 else (0,))]
+
+
+def sharded_batch(dev, world, rank, steps, warmup, barrier, sha) -> dict:
+    """The 96-instance batched configuration on every rank of the job: the
+    instances are sharded by voxel count (shard.partition_lpt), each rank solves
+    its share as one device-resident batch replayed from a CUDA graph, checks
+    each of its instances (flow and both cut sets) against the oracle's golden
+    answer, and the flows of all instances are gathered on every rank
+    (shard.solve_sharded).  Whole-job voxels/s over the max time over ranks."""
+    import torch
+    import torch.distributed as dist
+    from cugip_b200 import volume
+    from cugip_b200.graph_cut import Batch, Policy
+    from cugip_b200.shard import solve_sharded
+    n = 96
+    specs = [volume.preset(4, i) for i in range(n)]
+    extents = [(sp.X, sp.Y, sp.Z) for sp in specs]
+    gold = [golden(4, i) for i in range(n)]
+    st = {}
+
+    def check(idx, fl, outs):
+        for k, i in enumerate(idx):
+            if gold[i] is None:
+                continue
+            if fl[k] != gold[i]["flow"]:
+                raise SystemExit(f"sharded batch: instance {i} flow {fl[k]} differs from the oracle's")
+            if sha(outs[k][0].cpu().numpy()) != gold[i]["smin_sha256"] or \
+                    sha(outs[k][1].cpu().numpy()) != gold[i]["treach_sha256"]:
+                raise SystemExit(f"sharded batch: instance {i} cut sets differ from the oracle's")
+
+    def solve_local(idx):
+        vols = [volume.generate(specs[i]) for i in idx]
+        ins = [[torch.from_numpy(a).to(dev) for a in v.arrays()] for v in vols]
+        outs = [torch.zeros((2, v.N), dtype=torch.uint8, device=dev) for v in vols]
+        B = Batch([extents[i] for i in idx])
+        for k, (d, o) in enumerate(zip(ins, outs)):
+            B.bind_inputs(k, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
+            B.bind_outputs(k, o[0].data_ptr(), o[1].data_ptr())
+        best, _ = B.autotune([Policy(**c) for c in BATCH_CANDIDATES], repeats=1)
+        B.graph_create(best)
+        B.graph_launch()
+        fl = B.wait()
+        check(idx, fl, outs)
+        st.update(B=B, ins=ins, outs=outs, idx=idx, best=best, voxels=sum(v.N for v in vols))
+        return fl
+
+    flows = solve_sharded(extents, solve_local)
+    if any(g is not None and f != g["flow"] for f, g in zip(flows, gold)):
+        raise SystemExit("sharded batch: gathered flows differ from the oracle's")
+    B = st["B"]
+    for _ in range(max(3, warmup)):
+        B.graph_launch()
+        B.wait()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        B.graph_launch()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / steps
+    for o in st["outs"]:
+        o.fill_(7)
+    B.graph_launch()
+    check(st["idx"], B.wait(), st["outs"])
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+    total = sum(x * y * z for x, y, z in extents)
+    B.close()
+    return {"ms": ms, "voxels_per_s": total / ms * 1e3, "voxels": total, "instances": n, "ranks": world,
+            "rank0_instances": len(st["idx"]), "rank0_voxels": st["voxels"], "rank0_schedule": repr(st["best"]),
+            "parity": "oracle (each rank checks its instances' flows and both cut sets)"}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -466,6 +547,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e, ms_e2e_serial = float(t[0]), float(t[1]), float(t[2])
 
+    sharded = sharded_batch(dev, world, rank, args.steps, args.warmup, barrier, sha)
+
     line = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -500,6 +583,7 @@ def main():
                                                 "sched_ms")},
             "flow": int(flow),
             "clocks": clocks,
+            "batch96_sharded": sharded,
         }
 
     # ---- variants: plain vs tuned vs learned, single grid and batch
@@ -582,9 +666,7 @@ def main():
         for i, (d, o) in enumerate(zip(dins, douts)):
             BB.bind_inputs(i, d[0].data_ptr(), d[1].data_ptr(), [t.data_ptr() for t in d[2:]])
             BB.bind_outputs(i, o[0].data_ptr(), o[1].data_ptr())
-        bcands = [Policy(local_pulses=L, region_relabels=R, sweeps_per_relabel=K, ctas_per_sm=c, bfs_warp_min=bw)
-                  for (L, R, K) in ((4, 2, 8), (2, 4, 4), (2, 4, 8), (4, 2, 4), (4, 4, 8), (8, 2, 8)) for c in (2, 3, 4)
-                  for bw in ((0, 8) if c > 2 else (0,))]
+        bcands = [Policy(**c) for c in BATCH_CANDIDATES]
         bbest, _ = BB.autotune(bcands, repeats=1)
 
         def time_batch(pol, reps=3):
