@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcgc.so")
+# CGC_LIBRARY may name another build of the same ABI (the bounds-checked
+# libcgc_bounds.so for test runs)
+LIB_PATH = os.environ.get("CGC_LIBRARY") or os.path.join(HERE, "libcgc.so")
 
 CGC_OK = 0
 ERRORS = {

@@ -14,6 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcgc.so")
+# the same engine with every tile / neighbour / worklist index checked (CGC_BOUNDS_CHECK)
+BOUNDS_LIB = os.path.join(HERE, "libcgc_bounds.so")
 # synthetic workloads: host code only, so that CPU-only callers need no CUDA library
 VOL_LIB = os.path.join(HERE, "libcgcvol.so")
 VOL_SOURCES = ["cgc_volume.cpp"]
@@ -57,21 +59,25 @@ def build_volume(force: bool = False, verbose: bool = False) -> str:
     return VOL_LIB
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None, bounds_check: bool = False) -> str:
+    """Builds libcgc.so (or, with bounds_check, libcgc_bounds.so: the same
+    sources with -DCGC_BOUNDS_CHECK, for test runs only)."""
     build_volume(force, verbose)
+    lib = BOUNDS_LIB if bounds_check else LIB
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(INCLUDE, "cgc.h"), __file__]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, *(extra or []), "-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp",
+    if not force and not _stale(lib, deps):
+        return lib
+    flags = ["-DCGC_BOUNDS_CHECK"] if bounds_check else []
+    cmd = [_nvcc(), *NVCC_FLAGS, *flags, *(extra or []), "-I", INCLUDE, "-I", CSRC, "-o", lib + ".tmp",
            *[os.path.join(CSRC, s) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True,
-          extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else None)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose=True,
+                extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else None,
+                bounds_check="--bounds-check" in sys.argv))

@@ -45,7 +45,8 @@ enum Counter {
 // statistics in DevPool::stats (unsigned long long)
 enum Stat {
   S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5,
-  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_TRACE_CYC = 10, S_NS_SCHED = 11, S_NSTATS = 12
+  S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_TRACE_CYC = 10, S_NS_SCHED = 11,
+  S_BOUND_AT = 12 /* bounds-checked build: the first index found out of range */, S_NSTATS = 13
 };
 
 // phase trace records written by the persistent solve (two words each):

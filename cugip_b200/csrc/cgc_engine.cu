@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(512, 2) k_sweep_list(DevPool P, const int32_t*
 __global__ void k_compact(DevPool P, int parity, int32_t* list, int32_t* cnt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const bool pred = t < P.T && P.act[t] && P.tpar[t] == parity;
-  warp_append(pred, t, list, cnt);
+  warp_append(P, pred, t, list, cnt);
 }
 
 __global__ void __launch_bounds__(512) k_bfs_init(DevPool P) {
@@ -317,6 +317,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
   __shared__ int s_next;
   int round_no = 0;
   auto for_entries = [&](int n, auto&& visit) {
+    if (!CGC_IN_BOUNDS(P, n, P.T + 1)) n = P.T;  // a list holds at most T entries
     int32_t* take = P.cnt + C_TAKE0 + round_no % 3;
     if (b == 0 && tid == 0) P.cnt[C_TAKE0 + (round_no + 1) % 3] = 0;
     ++round_no;
@@ -373,8 +374,9 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     if (!grid_sync(P, prm.limit_ns)) return;
     int k = 0;
     for (;;) {
-      const int n = ld_cnt(bc + k % 3);
+      int n = ld_cnt(bc + k % 3);
       if (n == 0) break;
+      if (!CGC_IN_BOUNDS(P, n, P.T + 1)) n = P.T;  // a list holds at most T entries
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
       if (BFSW && n / G >= prm.bfs_warp_min) {
         // Throughput-bound round: a warp per tile (no block barriers, a
@@ -413,8 +415,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const bool a = t < P.T && __ldcg(P.act + t);
       const int par = a ? __ldcg(P.tpar + t) : 0;
       if (a) P.stamp_sw[t] = (uint32_t)(s + par + 1);
-      warp_append(a && par == 0, t, sl[s & 3], sc + (s & 3));
-      warp_append(a && par == 1, t, sl[(s + 1) & 3], sc + ((s + 1) & 3));
+      warp_append(P, a && par == 0, t, sl[s & 3], sc + (s & 3));
+      warp_append(P, a && par == 1, t, sl[(s + 1) & 3], sc + ((s + 1) & 3));
     }
     if (!grid_sync(P, prm.limit_ns)) return;
     const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));
@@ -639,6 +641,15 @@ int check_device_error(Pool& p, const char* where) {
   CGC_CUDA(cudaMemcpyAsync(&err, p.dp.err, sizeof(int32_t), cudaMemcpyDeviceToHost, p.stream));
   CGC_CUDA(cudaStreamSynchronize(p.stream));
   if (err == 0) return CGC_OK;
+#ifdef CGC_BOUNDS_CHECK
+  if (err == CGC_ERR_ARG) {
+    unsigned long long at = 0;
+    CGC_CUDA(cudaMemcpyAsync(&at, p.dp.stats + S_BOUND_AT, 8, cudaMemcpyDeviceToHost, p.stream));
+    CGC_CUDA(cudaStreamSynchronize(p.stream));
+    return fail(err, std::string(where) + ": index out of range (bounds-checked build): " +
+                         std::to_string((long long)at) + ", or a negative capacity");
+  }
+#endif
   const char* what = err == CGC_ERR_OVERFLOW ? "capacities may overflow int32 excess/residuals (or a capacity points outside the grid)"
                    : err == CGC_ERR_ARG ? "negative capacity"
                    : err == CGC_ERR_TIMEOUT ? "a device-side wait timed out"

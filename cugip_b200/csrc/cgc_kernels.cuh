@@ -69,6 +69,23 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 __device__ __forceinline__ void raise_error(const DevPool& P, int code) { atomicCAS(P.err, 0, code); }
 
+// Bounds-checked build (-DCGC_BOUNDS_CHECK; cugip_b200/build.py --bounds-check
+// builds libcgc_bounds.so): every tile, neighbour-tile and worklist index the
+// tile routines compute is checked against its array.  An index out of range
+// records CGC_ERR_ARG in the error word (the first one also its value in
+// stats[S_BOUND_AT]) and the access is skipped; nothing traps.  The product
+// build compiles the checks out.
+#ifdef CGC_BOUNDS_CHECK
+static __device__ __noinline__ bool bound_fail(const DevPool& P, long long i) {
+  if (atomicCAS(P.err, 0, CGC_ERR_ARG) == 0) P.stats[S_BOUND_AT] = (unsigned long long)i;
+  return false;
+}
+#define CGC_IN_BOUNDS(P, i, lim) \
+  ((long long)(i) >= 0 && (long long)(i) < (long long)(lim) ? true : ::cgc::bound_fail((P), (long long)(i)))
+#else
+#define CGC_IN_BOUNDS(P, i, lim) true
+#endif
+
 // Face f of the halo: thread k in [0,64) of face f writes halo entry (a,b) of
 // that face from the neighbouring tile (INF outside the grid).
 template <typename F>
@@ -91,14 +108,15 @@ __device__ __forceinline__ void for_halo_entry(int l, F&& fn) {
 __device__ __forceinline__ void load_halo_heights(const DevPool& P, int t, int (*sh)[HALO]) {
   for_halo_entry(threadIdx.x, [&](int f, int hi, int src) {
     const int nt = __ldcg(P.nbr + f * P.T + t);
-    const int v = (nt >= 0) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
+    const int v = (nt >= 0 && CGC_IN_BOUNDS(P, nt, P.T)) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
     sh[0][hi] = v;
     sh[1][hi] = v;
   });
 }
 
 // warp-aggregated append of `pred` items to list/cnt
-__device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t* list, int32_t* cnt) {
+// (worklists hold at most T entries: stamps let a tile in once per list)
+__device__ __forceinline__ void warp_append(const DevPool& P, bool pred, int32_t item, int32_t* list, int32_t* cnt) {
   const unsigned mask = __ballot_sync(0xffffffffu, pred);
   if (!mask) return;
   const int lane = threadIdx.x & 31;
@@ -106,12 +124,17 @@ __device__ __forceinline__ void warp_append(bool pred, int32_t item, int32_t* li
   int base = 0;
   if (lane == leader) base = atomicAdd(cnt, __popc(mask));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (pred) list[base + __popc(mask & ((1u << lane) - 1))] = item;
+  const int k = base + __popc(mask & ((1u << lane) - 1));
+  if (pred && CGC_IN_BOUNDS(P, k, P.T)) list[k] = item;
 }
 
 __device__ __forceinline__ void queue_tile(const DevPool& P, uint32_t* stamp, int t, uint32_t id, int32_t* list,
                                            int32_t* cnt) {
-  if (atomicExch(stamp + t, id) != id) list[atomicAdd(cnt, 1)] = t;
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;
+  if (atomicExch(stamp + t, id) != id) {
+    const int k = atomicAdd(cnt, 1);
+    if (CGC_IN_BOUNDS(P, k, P.T)) list[k] = t;
+  }
 }
 
 
@@ -171,6 +194,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
                            const SweepExtra ex = SweepExtra()) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
   const int64_t g = (int64_t)t * TV + l;
@@ -299,6 +323,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
     if (a > 0) {
       const int nt = S.nb[f];
       if (nt < 0) { raise_error(P, CGC_ERR_OVERFLOW); return; }  // capacity leaving the grid
+      if (!CGC_IN_BOUNDS(P, nt, P.T)) return;
       const int64_t ng = (int64_t)nt * TV + src;
       atomicAdd(P.e + ng, a);
       atomicAdd(P.r + (f ^ 1) * Np + ng, a);
@@ -329,7 +354,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
   // the tile re-queues itself from another warp than thread 0's face chain,
   // so the two dependent atomic chains overlap
   if (APPEND && l == 32 && still) queue_tile(P, P.stamp_sw, t, id_self, list_self, cnt_self);
-  if (l < 6 && ((S.flags >> l) & 1)) {
+  if (l < 6 && ((S.flags >> l) & 1) && CGC_IN_BOUNDS(P, S.nb[l], P.T)) {
     const int nt = S.nb[l];
     P.act[nt] = 1;
     if (APPEND) queue_tile(P, P.stamp_sw, nt, id_next, list_next, cnt_next);
@@ -357,6 +382,7 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
 // 16-byte stores into the tile-blocked planes.
 __device__ __forceinline__ void put_tile4(const DevPool& P, const int t, const int32_t* const* ip) {
   __shared__ long long red[4];
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
   const int inst = P.tinst[t];
   const InstGeo G = P.geo[inst];
   const int lt = t - G.tile_base;
@@ -526,7 +552,8 @@ __device__ __forceinline__ bool bfs_seed_tile(const DevPool& P, const int t) {
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         const int nt = __ldcg(P.nbr + d * P.T + t);
-        if (nt >= 0 && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1)) q = true;  // dead tiles have no seed bits
+        if (nt >= 0 && CGC_IN_BOUNDS(P, nt, P.T) && ((__ldcg(P.tflag + nt) >> (1 + (d ^ 1))) & 1))
+          q = true;  // dead tiles have no seed bits
       }
     }
   }
@@ -537,13 +564,14 @@ __device__ __forceinline__ void bfs_queue_tile(const DevPool& P, const int t, co
                                                int32_t* cnt0) {
   const bool q = bfs_seed_tile(P, t);
   if (q) P.stamp_bfs[t] = id0;
-  warp_append(q, t, list0, cnt0);
+  warp_append(P, q, t, list0, cnt0);
 }
 
 // One BFS visit: relax h(v) = min(h(v), 1 + h(u)) over residual edges v->u
 // until the tile is stable; re-queue face neighbours whose halo changed.
 __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
                          int32_t* list_next, int32_t* cnt_next) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the block; nothing can change
   const int l = threadIdx.x;
   const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
@@ -590,6 +618,7 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
 // (a warp per tile).
 __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S, const uint32_t id_next,
                            int32_t* list_next, int32_t* cnt_next) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
   const int l = threadIdx.x;
   const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
@@ -602,7 +631,7 @@ __device__ inline void reach_tile(const DevPool& P, const int t, ReachShared& S,
   for_halo_entry(l, [&](int f, int hh, int src) {
     const int nt = __ldcg(P.nbr + f * P.T + t);
     unsigned char rv = 0, mv = 0;
-    if (nt >= 0) {
+    if (nt >= 0 && CGC_IN_BOUNDS(P, nt, P.T)) {
       rv = __ldcg(P.reach + (int64_t)nt * TV + src);
       mv = __ldcg(P.rmask + (int64_t)nt * TV + src);
     }

@@ -33,7 +33,7 @@ __device__ __forceinline__ void warp_load_halo_heights(const DevPool& P, int t, 
   for (int m = 0; m < 12; ++m) {
     for_halo_entry(lane + 32 * m, [&](int f, int hi, int src) {
       const int nt = __ldcg(P.nbr + f * P.T + t);
-      sh[hi] = (nt >= 0) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
+      sh[hi] = (nt >= 0 && CGC_IN_BOUNDS(P, nt, P.T)) ? __ldcg(P.h + (int64_t)nt * TV + src) : INF;
     });
   }
 }
@@ -48,6 +48,7 @@ __device__ __forceinline__ void warp_load_halo_heights(const DevPool& P, int t, 
 // the first relabel of a solve.  A tile whose voxels are all seeds is final
 // at h = 1 and is never visited.
 __device__ inline void bfs_init_tile_w(const DevPool& P, const int t) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the warp
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
   bool dead = true, all_seed = true, any_excess = false;
@@ -85,6 +86,7 @@ __device__ inline void bfs_init_tile_w(const DevPool& P, const int t) {
 
 __device__ inline void bfs_tile_w(const DevPool& P, const int t, WarpBfsSmem& S, const uint32_t id_next,
                                   int32_t* list_next, int32_t* cnt_next) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;      // uniform over the warp
   if (__ldcg(P.tflag + t) & TF_DEAD) return;  // uniform over the warp
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
@@ -147,6 +149,7 @@ __device__ inline void bfs_tile_w(const DevPool& P, const int t, WarpBfsSmem& S,
 // if it has one, and so is every face neighbour next to one.
 __device__ inline void reach_init_tile_w(const DevPool& P, const int t, const uint32_t id0, int32_t* list0,
                                          int32_t* cnt0) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the warp
   const int lane = threadIdx.x & 31;
   const int64_t base = (int64_t)t * TV;
   // A seed only spreads along its residual edges: the tile needs a visit if
