@@ -110,6 +110,7 @@ SIGNATURES = {
     "cgc_autotune_lookup": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(Options)]),
     "cgc_scheduler_load": (C.c_int, [VP, VP]),
     "cgc_scheduler_load_file": (C.c_int, [C.c_char_p]),
+    "cgc_scheduler_infer": (C.c_int, [C.c_int32, C.c_int32, VP, VP, VP, VP, VP]),
     "cgc_grid_sched_trace": (C.c_int, [VP, VP, VP, VP, C.c_int32, P32]),
     "cgc_trainer_create": (C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(VP)]),
     "cgc_trainer_destroy": (C.c_int, [VP]),

@@ -97,11 +97,10 @@ struct DevPool {
   __nv_bfloat16* sfeat;       // T*16 tile features
   __nv_bfloat16* sact0;       // T*16 activations of conv 1
   __nv_bfloat16* sact1;       // T*16 activations of conv 2
-  const __nv_bfloat16* swconv;  // 3 layers * 27 taps * 16 * 16
+  const uint2* swfrag;        // 3 layers of convolution weights in mma fragment order (cgc_sched.cuh)
   const float* swhead;        // 2*16 weights + 2 biases
   uint8_t* sbudget;           // T: pulses per visit until the next relabel
   uint8_t* sprio;             // T: 1 = high priority
-  uint8_t* smask;             // T: region mask of the CNN stages (SchedMask bits)
   // scheduling traces for training (null unless recorded)
   __nv_bfloat16* tfeat;       // cycles*T*16 features at the start of each relabel cycle
   uint8_t* tpulses;           // cycles*T: pulses of the tile's first visit in the cycle (0 = not visited)

@@ -237,53 +237,33 @@ __device__ __forceinline__ bool grid_sync(const DevPool& P, uint64_t limit_ns) {
 __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile const int32_t*)p; }
 
 
-// Learned-scheduler stage at the start of a relabel cycle: region masks,
-// features, three convolution layers and the head (budgets and priorities
-// of the active tiles); with `tracing`, the features are also recorded.
-// Returns false when a barrier failed.
-__device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams& prm, int cycle, bool learned, bool tracing) {
-  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
-  // stage 0: region mask (active tiles) and, when tracing, cleared trace rows
-  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
-    P.smask[t] = __ldcg(P.act + t) ? (uint8_t)(SM_ACTIVE | SM_L3) : (uint8_t)0;
-    if (tracing) {
-      const int64_t r = (int64_t)cycle * P.T + t;
-      P.tpulses[r] = 0;
-      P.tsink[r] = 0;
-#pragma unroll
-      for (int c = 0; c < SCHED_C; ++c) P.tfeat[r * SCHED_C + c] = __float2bfloat16(0.f);
-    }
-  }
-  if (!grid_sync(P, prm.limit_ns)) return false;
-  // stage 1: features of the active tiles (warp per tile), mask dilation
+// Learned-scheduler stage at the start of a relabel cycle: the features of
+// every tile (zero for inactive ones; recorded when tracing), then the three
+// convolution layers on the tensor cores, the last one with the head (budgets
+// and priorities).  Four grid barriers.  Returns false when a barrier failed.
+__device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams& prm, int cycle, bool learned,
+                                            bool tracing, SchedShared& sh) {
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
   const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
   for (int t = gw; t < P.T; t += nw) {
-    if (!(__ldcg(P.smask + t) & SM_ACTIVE)) continue;
-    sched_features_warp(P, t, P.sfeat);
-    if (tracing && (tid & 31) < SCHED_C) {
-      const int c = tid & 31;
-      P.tfeat[((int64_t)cycle * P.T + t) * SCHED_C + c] = P.sfeat[(int64_t)t * SCHED_C + c];
+    if (__ldcg(P.act + t)) {
+      sched_features_warp(P, t, P.sfeat);
+    } else if (lane < 8) {
+      reinterpret_cast<uint32_t*>(P.sfeat)[(int64_t)t * 8 + lane] = 0u;
     }
-  }
-  if (!learned) return grid_sync(P, prm.limit_ns);
-  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L3, SM_L2);
-  if (!grid_sync(P, prm.limit_ns)) return false;
-  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L2, SM_L1);
-  if (!grid_sync(P, prm.limit_ns)) return false;
-  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) sched_dilate(P, t, SM_L1, SM_FEAT);
-  if (!grid_sync(P, prm.limit_ns)) return false;
-  // inactive tiles that conv 1 reads hold zero features
-  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
-    const unsigned m = __ldcg(P.smask + t);
-    if ((m & SM_FEAT) && !(m & SM_ACTIVE)) {
-      uint4* f = reinterpret_cast<uint4*>(P.sfeat + (int64_t)t * SCHED_C);
-      f[0] = make_uint4(0, 0, 0, 0);
-      f[1] = make_uint4(0, 0, 0, 0);
+    if (tracing) {
+      __syncwarp();
+      const int64_t r = (int64_t)cycle * P.T + t;
+      if (lane < 8)
+        reinterpret_cast<uint32_t*>(P.tfeat)[r * 8 + lane] = __ldcg(reinterpret_cast<const uint32_t*>(P.sfeat) + t * 8 + lane);
+      if (lane == 0) { P.tpulses[r] = 0; P.tsink[r] = 0; }
     }
   }
   if (!grid_sync(P, prm.limit_ns)) return false;
+  if (!learned) return true;
+  const PoolSpace sp{&P};
   for (int layer = 0; layer < 3; ++layer) {
-    sched_layer(P, layer, gw, nw);
+    sched_layer(sp, layer, pool_io(P, layer), gw, nw, nullptr);
     if (!grid_sync(P, prm.limit_ns)) return false;
   }
   return true;
@@ -441,7 +421,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     // fewer, a sweep lasts one tile visit whatever the order or budgets.
     const bool learned = prm.learned && nact > 2 * G;
     if (learned || tracing) {
-      if (!sched_stage(P, prm, cycle, learned, tracing)) return;
+      if (!sched_stage(P, prm, cycle, learned, tracing, S.sched)) return;
       lap(ns_sched);
     }
     // ------------------------------------------------ sweeps

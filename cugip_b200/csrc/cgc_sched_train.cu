@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -34,30 +35,48 @@ uint64_t g_wver = 0;            // 0: nothing loaded
 
 }  // namespace
 
+// The convolution weights ([layer][tap][cin][cout] BF16 bits) as the B
+// fragments of mma.sync.m16n8k16 ([layer][tap][half][lane] -> 2 registers):
+// register 0 holds cin 2q, 2q+1 and register 1 cin 2q+8, 2q+9 of output
+// channel 8*half + g (g = lane / 4, q = lane % 4), lower cin in the low half.
+std::vector<uint32_t> fragment_order(const std::vector<uint16_t>& w) {
+  std::vector<uint32_t> f((size_t)3 * SCHED_FRAG * 2);
+  for (int l = 0; l < 3; ++l)
+    for (int k = 0; k < SCHED_TAPS; ++k)
+      for (int h = 0; h < 2; ++h)
+        for (int lane = 0; lane < 32; ++lane) {
+          const int g = lane >> 2, q = lane & 3, co = 8 * h + g;
+          auto wv = [&](int ci) -> uint32_t { return w[(size_t)l * SCHED_WCONV + (k * SCHED_C + ci) * SCHED_C + co]; };
+          const size_t at = (((size_t)l * SCHED_TAPS + k) * 2 + h) * 32 + lane;
+          f[2 * at] = wv(2 * q) | (wv(2 * q + 1) << 16);
+          f[2 * at + 1] = wv(2 * q + 8) | (wv(2 * q + 9) << 16);
+        }
+  return f;
+}
+
 // Device buffers of the scheduler for one pool (allocated on first use).
 int ensure_sched(Pool& p, bool learned, int trace_cycles) {
   DevPool& d = p.dp;
   const int64_t T = d.T;
   if (!p.sbuf) {
-    const size_t bytes = (size_t)3 * T * SCHED_C * 2 + (size_t)3 * SCHED_WCONV * 2 + SCHED_NHEAD * 4 + 3 * (size_t)T + 512;
+    const size_t bytes = (size_t)3 * T * SCHED_C * 2 + (size_t)3 * SCHED_FRAG * 8 + SCHED_NHEAD * 4 + 2 * (size_t)T;
     CGC_CUDA(cudaMalloc(&p.sbuf, bytes));
     CGC_CUDA(cudaMemset(p.sbuf, 0, bytes));
     char* q = (char*)p.sbuf;
     d.sfeat = (__nv_bfloat16*)q; q += (size_t)T * SCHED_C * 2;
     d.sact0 = (__nv_bfloat16*)q; q += (size_t)T * SCHED_C * 2;
     d.sact1 = (__nv_bfloat16*)q; q += (size_t)T * SCHED_C * 2;
-    d.swconv = (const __nv_bfloat16*)q; q += (size_t)3 * SCHED_WCONV * 2;
+    d.swfrag = (const uint2*)q; q += (size_t)3 * SCHED_FRAG * 8;
     d.swhead = (const float*)q; q += SCHED_NHEAD * 4;
     d.sbudget = (uint8_t*)q; q += T;
-    d.sprio = (uint8_t*)q; q += T;
-    q = (char*)(((uintptr_t)q + 255) & ~(uintptr_t)255);  // word-aligned for atomicOr
-    d.smask = (uint8_t*)q;
+    d.sprio = (uint8_t*)q;
   }
   if (learned) {
     std::lock_guard<std::mutex> lock(g_wmu);
     if (!g_wver) return fail(CGC_ERR_STATE, "learned scheduler requested but no weights are loaded (cgc_scheduler_load)");
     if (p.sched_wver != g_wver) {
-      CGC_CUDA(cudaMemcpy((void*)d.swconv, g_wconv.data(), g_wconv.size() * 2, cudaMemcpyHostToDevice));
+      const std::vector<uint32_t> frag = fragment_order(g_wconv);
+      CGC_CUDA(cudaMemcpy((void*)d.swfrag, frag.data(), frag.size() * 4, cudaMemcpyHostToDevice));
       CGC_CUDA(cudaMemcpy((void*)d.swhead, g_whead.data(), g_whead.size() * 4, cudaMemcpyHostToDevice));
       p.sched_wver = g_wver;
     }
@@ -285,6 +304,15 @@ static int trainer_forward_backward(Trainer& tr, int grids, const uint16_t* feat
 
 }  // namespace cgc
 
+namespace cgc {
+namespace {
+__global__ void __launch_bounds__(256) k_infer_layer(GridSpace sp, int layer, SchedIO io) {
+  sched_layer(sp, layer, io, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), gridDim.x * (blockDim.x >> 5),
+              nullptr);
+}
+}  // namespace
+}  // namespace cgc
+
 struct cgc_trainer { cgc::Trainer t; };
 
 extern "C" {
@@ -311,6 +339,52 @@ int cgc_scheduler_load_file(const char* path) {
   std::fclose(f);
   if (!okr) return cgc::fail(CGC_ERR_ARG, std::string("not a scheduler weight file: ") + path);
   return cgc_scheduler_load(conv.data(), head.data());
+}
+
+int cgc_scheduler_infer(int32_t grids, int32_t D, const uint16_t* feat, uint8_t* budget, uint8_t* prio, float* logits,
+                        void* stream) {
+  using namespace cgc;
+  if (grids <= 0 || D <= 0 || !feat || !budget || !prio) return fail(CGC_ERR_ARG, "cgc_scheduler_infer: bad arguments");
+  std::vector<uint32_t> frag;
+  std::vector<float> head;
+  {
+    std::lock_guard<std::mutex> lock(g_wmu);
+    if (!g_wver) return fail(CGC_ERR_STATE, "cgc_scheduler_infer: no weights are loaded (cgc_scheduler_load)");
+    frag = fragment_order(g_wconv);
+    head = g_whead;
+  }
+  const int64_t T = (int64_t)grids * D * D * D;
+  if (T > (int64_t)1 << 30) return fail(CGC_ERR_ARG, "cgc_scheduler_infer: too many tiles");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* buf = nullptr;
+  const size_t act_bytes = (size_t)T * SCHED_C * 2;
+  CGC_CUDA(cudaMalloc(&buf, 2 * act_bytes + frag.size() * 4 + head.size() * 4));
+  auto release = [&]() { cudaFree(buf); };
+  uint32_t* a0 = reinterpret_cast<uint32_t*>(buf);
+  uint32_t* a1 = reinterpret_cast<uint32_t*>(buf + act_bytes);
+  uint2* wf = reinterpret_cast<uint2*>(buf + 2 * act_bytes);
+  float* wh = reinterpret_cast<float*>(buf + 2 * act_bytes + frag.size() * 4);
+  cudaError_t e = cudaMemcpyAsync(wf, frag.data(), frag.size() * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(wh, head.data(), head.size() * 4, cudaMemcpyHostToDevice, st);
+  const GridSpace sp{grids, D};
+  const unsigned blocks = (unsigned)std::min<int64_t>((T + 127) / 128, 8192);
+  for (int layer = 0; layer < 3 && e == cudaSuccess; ++layer) {
+    SchedIO io{};
+    io.in = layer == 0 ? reinterpret_cast<const uint32_t*>(feat) : (layer == 1 ? a0 : a1);
+    io.out = layer == 0 ? a0 : a1;
+    io.wf = wf + (size_t)layer * SCHED_FRAG;
+    io.wh = wh;
+    io.budget = budget;
+    io.prio = prio;
+    io.logits = logits;
+    k_infer_layer<<<blocks, 256, 0, st>>>(sp, layer, io);
+    note_launch();
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return fail(CGC_ERR_CUDA, std::string("cgc_scheduler_infer: ") + cudaGetErrorString(e));
+  return ok();
 }
 
 int cgc_trainer_create(int32_t max_grids, int32_t D, uint64_t seed, cgc_trainer** out) {

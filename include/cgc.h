@@ -307,6 +307,12 @@ int cgc_autotune_lookup(int64_t voxels, int32_t instances, cgc_options* out);
  * 8-byte tag "CGCSCHD1" followed by both arrays. */
 int cgc_scheduler_load(const uint16_t* conv_bf16, const float* head);
 int cgc_scheduler_load_file(const char* path);
+/* The CNN of the loaded weights on stacks of D^3 tile grids (device arrays:
+ * feat grids*D^3*16 BF16 features, x fastest; budget and prio one byte per
+ * tile; logits, may be NULL, the head's two logits per tile), with the same
+ * tensor-core kernels the solve runs.  For tests and tools. */
+int cgc_scheduler_infer(int32_t grids, int32_t D, const uint16_t* feat, uint8_t* budget, uint8_t* prio, float* logits,
+                        void* stream);
 /* Scheduling traces of the last solve run with cgc_options.trace_cycles > 0:
  * for each recorded relabel cycle c and tile t (tile order of the grid,
  * x fastest), feat[(c*T + t)*16 + k] (BF16 features), pulses[c*T + t] (pulses
