@@ -334,6 +334,23 @@ def _bk_worker(workload: int) -> float:
     return oracle.maxflow_grid(v.X, v.Y, v.Z, v.capS, v.capT, v.n, algo=oracle.BK)[3]
 
 
+def reference_processes(voxels: int) -> int:
+    """Concurrent single-threaded BK solves for the CPU arm: every core this
+    process may run on, as far as host memory holds one solve per process
+    (about 150 bytes per voxel at peak: volume, graph, trees and queues)."""
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = None
+    by_mem = max(1, int(0.7 * avail / (150 * voxels))) if avail else cores
+    return max(1, min(cores, by_mem))
+
+
 def run_reference(args, rank: int, world: int):
     """CPU reference arm: the oracle's BK port on the host cores (replicas of the
     workload solved concurrently by independent processes)."""
@@ -342,7 +359,7 @@ def run_reference(args, rank: int, world: int):
     import multiprocessing as mp
     from cugip_b200 import volume
     v = volume.workload(args.workload)
-    procs = max(1, min(os.cpu_count() or 1, 8))
+    procs = reference_processes(v.N)
     ctx = mp.get_context("spawn")
     times = []
     with ctx.Pool(procs) as pool:
