@@ -246,18 +246,14 @@ __device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams&
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
   const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
   for (int t = gw; t < P.T; t += nw) {
+    const int64_t r = (int64_t)cycle * P.T + t;  // trace row
     if (__ldcg(P.act + t)) {
-      sched_features_warp(P, t, P.sfeat);
+      sched_features_warp(P, t, P.sfeat, tracing ? P.tfeat + r * SCHED_C : nullptr);
     } else if (lane < 8) {
       reinterpret_cast<uint32_t*>(P.sfeat)[(int64_t)t * 8 + lane] = 0u;
+      if (tracing) reinterpret_cast<uint32_t*>(P.tfeat)[r * 8 + lane] = 0u;
     }
-    if (tracing) {
-      __syncwarp();
-      const int64_t r = (int64_t)cycle * P.T + t;
-      if (lane < 8)
-        reinterpret_cast<uint32_t*>(P.tfeat)[r * 8 + lane] = __ldcg(reinterpret_cast<const uint32_t*>(P.sfeat) + t * 8 + lane);
-      if (lane == 0) { P.tpulses[r] = 0; P.tsink[r] = 0; }
-    }
+    if (tracing && lane == 0) { P.tpulses[r] = 0; P.tsink[r] = 0; }
   }
   if (!grid_sync(P, prm.limit_ns)) return false;
   if (!learned) return true;

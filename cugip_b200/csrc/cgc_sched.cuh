@@ -63,8 +63,10 @@ __device__ __forceinline__ int tap_tile(const TileCoord& c, int k) {
   return c.base + x + c.TX * (y + c.TY * z);
 }
 
-// Features of active tile t by one warp (16 coalesced passes over its voxels).
-__device__ inline void sched_features_warp(const DevPool& P, const int t, __nv_bfloat16* out) {
+// Features of active tile t by one warp (16 coalesced passes over its voxels)
+// into out[t] and, if given, into trace row out2.
+__device__ inline void sched_features_warp(const DevPool& P, const int t, __nv_bfloat16* out,
+                                           __nv_bfloat16* out2 = nullptr) {
   const int lane = threadIdx.x & 31;
   unsigned long long ex = 0;
   int act = 0, bins[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -92,6 +94,7 @@ __device__ inline void sched_features_warp(const DevPool& P, const int t, __nv_b
         if (lane == 2 + k) v = (float)bins[k] * (1.0f / 512.0f);
     }
     out[(int64_t)t * SCHED_C + lane] = __float2bfloat16(v);
+    if (out2) out2[lane] = __float2bfloat16(v);
   }
 }
 
