@@ -37,7 +37,7 @@ class Options(C.Structure):
                 ("wait_limit_us", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
                 ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("learned", C.c_int32), ("trace_cycles", C.c_int32),
-                ("bfs_warp_min", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("bfs_warp_min", C.c_int32), ("exclusive", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Stats(C.Structure):
@@ -148,7 +148,8 @@ def check(rc: int) -> None:
 
 
 OPTION_FIELDS = ("local_pulses", "sweeps_per_relabel", "wait_limit_us", "max_sweeps", "persistent",
-                 "region_relabels", "stall_sweeps", "ctas_per_sm", "learned", "trace_cycles", "bfs_warp_min")
+                 "region_relabels", "stall_sweeps", "ctas_per_sm", "learned", "trace_cycles", "bfs_warp_min",
+                 "exclusive")
 
 
 def options(**fields) -> Options:

@@ -103,7 +103,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   CGC_CUDA(cudaMemsetAsync(d.err, 0, 4, stream));
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, stream));
-  CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, 2 * (size_t)d.T * 4, stream));
   k_put_all<<<d.T, 128, 0, stream>>>(d, p.d_in);
   note_launch();
   const SolveParams prm = solve_params(o);

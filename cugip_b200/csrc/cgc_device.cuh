@@ -84,7 +84,7 @@ struct DevPool {
   uint8_t* act;         // T: tile holds an active voxel (e>0, h<INF)
   uint16_t* tflag;      // T: BFS seed summary (TF_* bits)
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
-  uint32_t* stamp_sw;   // T: last sweep the tile was queued for
+  uint32_t* stamp_sw;   // 2*T: last sweep the tile was queued for (exclusive sweeps: half s&1 for sweep s)
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
   int32_t* cnt;         // C_NCOUNTERS
   unsigned long long* flow;   // ninst: flow value (int64 as two's complement)
@@ -118,6 +118,7 @@ struct SolveParams {
   int64_t max_sweeps;    // cap on sweeps (parity steps)
   uint64_t limit_ns;     // bounded barrier wait
   int bfs_warp_min = 0;  // BFS rounds with at least this many tiles per CTA run a warp per tile (0: never)
+  int exclusive = 0;     // 1: exclusive sweeps (cgc_options.exclusive), 0: parity sweeps
 };
 
 // kernels of cgc_engine.cu launched from other translation units

@@ -390,9 +390,14 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       const int t = t0 + (tid & 31);
       const bool a = t < P.T && __ldcg(P.act + t);
       const int par = a ? __ldcg(P.tpar + t) : 0;
-      if (a) P.stamp_sw[t] = (uint32_t)(s + par + 1);
-      warp_append(P, a && par == 0, t, sl[s & 3], sc + (s & 3));
-      warp_append(P, a && par == 1, t, sl[(s + 1) & 3], sc + ((s + 1) & 3));
+      if (prm.exclusive) {  // one list: the whole active set is queued for sweep s
+        if (a) P.stamp_sw[(s & 1) * P.T + t] = (uint32_t)(s + 1);
+        warp_append(P, a, t, sl[s & 3], sc + (s & 3));
+      } else {              // one list per parity, for sweeps s and s + 1
+        if (a) P.stamp_sw[t] = (uint32_t)(s + par + 1);
+        warp_append(P, a && par == 0, t, sl[s & 3], sc + (s & 3));
+        warp_append(P, a && par == 1, t, sl[(s + 1) & 3], sc + ((s + 1) & 3));
+      }
     }
     if (!grid_sync(P, prm.limit_ns)) return;
     const int nact = ld_cnt(sc + (s & 3)) + ld_cnt(sc + ((s + 1) & 3));
@@ -429,7 +434,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     int idle = 0;  // consecutive sweeps in which no tile delivered flow to the sink
     for (int j = 0; j < 2 * prm.K; ++j, ++s) {
       const int n = ld_cnt(sc + (s & 3));
-      if (n == 0 && ld_cnt(sc + ((s + 1) & 3)) == 0) break;
+      if (n == 0 && (prm.exclusive || ld_cnt(sc + ((s + 1) & 3)) == 0)) break;
       if (b == 0 && tid == 0) {
         sc[(s + 3) & 3] = 0;
         P.cnt[C_SINKT0 + (int)((s + 1) % 3)] = 0;
@@ -438,16 +443,39 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       // the learned scheduler defers low-priority tiles during the first half
       // of the cycle; every active tile is swept in the second half
       const bool may_defer = learned && prm.learned == 1 && j < prm.K;
+      // Parity sweeps: sweep s uses stamp id s + 1; a visited tile queues the
+      // tiles it pushed into for sweep s + 1 and itself, of the same parity,
+      // for sweep s + 2.  Exclusive sweeps: every queued tile runs unless it
+      // has the other parity than s and a face neighbour is queued for sweep
+      // s, so the tiles that run form an independent set (no two share a
+      // face) and the halo heights and cross-face pushes are exact as under
+      // the parity schedule; everything is queued for sweep s + 1, with the
+      // stamps in half (s+1)&1 of stamp_sw, so half s&1 -- this sweep's list --
+      // does not change during the sweep.
+      uint32_t* const stamp_q = prm.exclusive ? P.stamp_sw + ((s + 1) & 1) * P.T : P.stamp_sw;
+      const uint32_t id_self = (uint32_t)(prm.exclusive ? s + 2 : s + 3);
+      int32_t* const list_self = sl[(prm.exclusive ? s + 1 : s + 2) & 3];
+      int32_t* const cnt_self = sc + ((prm.exclusive ? s + 1 : s + 2) & 3);
       for_entries(n, [&](int i) {
         const int t = __ldcg(sl[s & 3] + i);
         if (may_defer && !__ldcg(P.sprio + t)) {
-          if (leader && atomicExch(P.stamp_sw + t, (uint32_t)(s + 3)) != (uint32_t)(s + 3))
-            sl[(s + 2) & 3][atomicAdd(sc + ((s + 2) & 3), 1)] = t;
+          if (leader && atomicExch(stamp_q + t, id_self) != id_self) list_self[atomicAdd(cnt_self, 1)] = t;
           return;
         }
+        if (prm.exclusive && (int)__ldcg(P.tpar + t) != (int)(s & 1)) {  // uniform over the block
+          bool queued_nb = false;
+          if (tid < 6) {
+            const int nb = __ldcg(P.nbr + tid * P.T + t);
+            queued_nb = nb >= 0 && __ldcg(P.stamp_sw + (s & 1) * P.T + nb) == (uint32_t)(s + 1);
+          }
+          if (__syncthreads_or(queued_nb)) {  // wait one sweep
+            if (leader) queue_tile(P, stamp_q, t, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3));
+            return;
+          }
+        }
         const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
-        sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3),
-                         (uint32_t)(s + 3), sl[(s + 2) & 3], sc + ((s + 2) & 3), ex);
+        sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3), id_self,
+                         list_self, cnt_self, ex, stamp_q);
       });
       ++sweeps;
       if (!grid_sync(P, prm.limit_ns)) return;
@@ -678,7 +706,7 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   const int64_t o_act = off; off += al(T);
   const int64_t o_tf = off; off += al(T * 2);
   const int64_t o_sb = off; off += al(T * 4);
-  const int64_t o_ss = off; off += al(T * 4);
+  const int64_t o_ss = off; off += al(2 * T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
   const int64_t o_cnt = off; off += al(C_NCOUNTERS * 4);
   const int64_t o_fl = off; off += al((int64_t)count * 8);
@@ -844,6 +872,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->stall_sweeps) r.stall_sweeps = o->stall_sweeps < 0 ? 0 : o->stall_sweeps;
     if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
     r.bfs_warp_min = o->bfs_warp_min > 0 ? o->bfs_warp_min : 0;
+    r.exclusive = o->exclusive > 0 ? 1 : 0;
     r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
@@ -866,6 +895,7 @@ SolveParams solve_params(const cgc_options& o) {
   prm.max_sweeps = (int64_t)o.max_sweeps;
   prm.limit_ns = wait_limit_ns(o);
   prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
+  prm.exclusive = o.exclusive ? 1 : 0;
   return prm;
 }
 
@@ -944,7 +974,7 @@ int pool_solve_async(Pool& p, const cgc_options* opts) {
   CGC_CUDA(cudaMemsetAsync(d.err, 0, 4, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, p.stream));
-  CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, (size_t)d.T * 4, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, 2 * (size_t)d.T * 4, p.stream));
   if (p.ninst == 1) {
     InputPlanes ip;
     for (int k = 0; k < 8; ++k) ip.p[k] = in[k];

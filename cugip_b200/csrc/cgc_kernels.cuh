@@ -189,11 +189,13 @@ struct SweepExtra {
   uint8_t* tr_sink = nullptr;     // trace: delivered sink flow in this cycle
 };
 
+//   stamp_q: the stamps the queued tiles get (null: P.stamp_sw).
 template <bool APPEND>
 __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, const int R, SweepShared& S,
                            const uint32_t id_next, int32_t* list_next, int32_t* cnt_next,
                            const uint32_t id_self, int32_t* list_self, int32_t* cnt_self,
-                           const SweepExtra ex = SweepExtra()) {
+                           const SweepExtra ex = SweepExtra(), uint32_t* stamp_q = nullptr) {
+  if (!stamp_q) stamp_q = P.stamp_sw;
   if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
   const int l = threadIdx.x;
   const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
@@ -353,11 +355,11 @@ __device__ inline void sweep_tile(const DevPool& P, const int t, const int L, co
   }
   // the tile re-queues itself from another warp than thread 0's face chain,
   // so the two dependent atomic chains overlap
-  if (APPEND && l == 32 && still) queue_tile(P, P.stamp_sw, t, id_self, list_self, cnt_self);
+  if (APPEND && l == 32 && still) queue_tile(P, stamp_q, t, id_self, list_self, cnt_self);
   if (l < 6 && ((S.flags >> l) & 1) && CGC_IN_BOUNDS(P, S.nb[l], P.T)) {
     const int nt = S.nb[l];
     P.act[nt] = 1;
-    if (APPEND) queue_tile(P, P.stamp_sw, nt, id_next, list_next, cnt_next);
+    if (APPEND) queue_tile(P, stamp_q, nt, id_next, list_next, cnt_next);
   }
   __syncthreads();
 }

@@ -194,6 +194,7 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   cgc_options o = resolve_options(opts);
   o.learned = 0;  // the learned scheduler and its traces need allocated buffers
   o.trace_cycles = 0;
+  o.exclusive = 0;  // the scratch holds one half of stamps
   const SolveParams prm = solve_params(o);
   void* args[] = {(void*)&P, (void*)&prm};
   // a preparation error (overflowing capacities) makes every CTA leave at its

@@ -78,7 +78,10 @@ typedef struct cgc_options {
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
   int32_t bfs_warp_min;       /* persistent, 3 or 4 CTAs/SM: BFS rounds with at least this many tiles per CTA
                                  visit a tile with one warp (0 = never, the default) */
-  int32_t reserved[4];
+  int32_t exclusive;          /* persistent: 1 = every sweep visits each queued tile, except a tile that has a
+                                 face neighbour of the sweep's parity queued for the same sweep (which waits one
+                                 sweep); 0 = checkerboard sweeps, one parity at a time (the default) */
+  int32_t reserved[3];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */

@@ -60,6 +60,7 @@ struct GraphCutPolicy {
   int ctas_per_sm = 0;         // 2 (default), 3 or 4 CTAs per SM
   int learned = 0;             // learned scheduler: 1 budgets + priorities, 2 budgets only
   int bfs_warp_min = 0;        // 3/4 CTAs per SM: BFS rounds with this many tiles per CTA use a warp per tile
+  int exclusive = 0;           // 1: sweeps visit every queued tile without a queued face neighbour of the sweep's parity
   cgc_options options() const {
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
@@ -73,6 +74,7 @@ struct GraphCutPolicy {
     o.ctas_per_sm = ctas_per_sm;
     o.learned = learned;
     o.bfs_warp_min = bfs_warp_min;
+    o.exclusive = exclusive;
     return o;
   }
   // The autotuner's choice for a size class (cgc_autotune_lookup), if any
@@ -91,6 +93,7 @@ struct GraphCutPolicy {
     out->ctas_per_sm = o.ctas_per_sm;
     out->learned = o.learned;
     out->bfs_warp_min = o.bfs_warp_min;
+    out->exclusive = o.exclusive;
     return true;
   }
 };

@@ -55,7 +55,8 @@ def test_ctypes_mirrors_match_the_c_structs(tmp_path):
 
 def test_python_policy_round_trip_keeps_every_field():
     values = dict(local_pulses=3, sweeps_per_relabel=5, wait_limit_us=1000, max_sweeps=77, persistent=-1,
-                  region_relabels=2, stall_sweeps=4, ctas_per_sm=3, learned=2, trace_cycles=6, bfs_warp_min=8)
+                  region_relabels=2, stall_sweeps=4, ctas_per_sm=3, learned=2, trace_cycles=6, bfs_warp_min=8,
+                  exclusive=1)
     p = Policy(**values)
     o = p.options()
     assert o.struct_size == C.sizeof(_lib.Options)
@@ -76,12 +77,12 @@ CPP = r"""
 int main() {
   cgc::GraphCutPolicy p;
   p.local_pulses = 3; p.region_relabels = 2; p.sweeps_per_relabel = 5; p.persistent = -1; p.wait_limit_us = 1000;
-  p.max_sweeps = 77; p.stall_sweeps = 4; p.ctas_per_sm = 3; p.learned = 2; p.bfs_warp_min = 8;
+  p.max_sweeps = 77; p.stall_sweeps = 4; p.ctas_per_sm = 3; p.learned = 2; p.bfs_warp_min = 8; p.exclusive = 1;
   const cgc_options o = p.options();
   EXPECT(o.struct_size == (int)sizeof(cgc_options));
   EXPECT(o.local_pulses == 3 && o.region_relabels == 2 && o.sweeps_per_relabel == 5 && o.persistent == -1);
   EXPECT(o.wait_limit_us == 1000 && o.max_sweeps == 77 && o.stall_sweeps == 4 && o.ctas_per_sm == 3);
-  EXPECT(o.learned == 2 && o.bfs_warp_min == 8 && o.trace_cycles == 0);
+  EXPECT(o.learned == 2 && o.bfs_warp_min == 8 && o.trace_cycles == 0 && o.exclusive == 1);
   // the cache file holds one choice for a single 256^3 grid
   cgc::GraphCutPolicy t;
   EXPECT(cgc::GraphCutPolicy::autotuned(256LL * 256 * 256, 1, &t));

@@ -56,7 +56,9 @@ def test_enqueue_matches_golden(device_batch):
                                     Policy(ctas_per_sm=3, stall_sweeps=1, sweeps_per_relabel=64),
                                     Policy(ctas_per_sm=4, region_relabels=-1, local_pulses=8),
                                     Policy(ctas_per_sm=4, region_relabels=4),
-                                    Policy(ctas_per_sm=4, region_relabels=4, bfs_warp_min=8)])
+                                    Policy(ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
+                                    Policy(exclusive=1, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
+                                    Policy(exclusive=1, local_pulses=2, sweeps_per_relabel=3)])
 def test_graph_replay_matches_golden(device_batch, policy):
     B, vols, ins, outs, flows = device_batch
     B.graph_create(policy, flows.data_ptr())
@@ -202,7 +204,9 @@ def test_outputs_at_unaligned_addresses(device_batch, offset):
 
 
 @pytest.mark.parametrize("policy", [None, Policy(local_pulses=2, region_relabels=4, sweeps_per_relabel=4, ctas_per_sm=4,
-                                                 bfs_warp_min=8)])
+                                                 bfs_warp_min=8),
+                                    Policy(exclusive=1, local_pulses=2, region_relabels=4, sweeps_per_relabel=4,
+                                           ctas_per_sm=4, bfs_warp_min=8)])
 def test_all_96_instances_match_the_oracle(policy):
     """The batched configuration itself: all 96 instances (extents 32..160)
     bound to one batch, the CUDA graph replayed twice, and every instance's

@@ -37,6 +37,10 @@ POLICIES = {
     "cta4_no_region": Policy(ctas_per_sm=4, region_relabels=-1, local_pulses=8),
     "cta3_stall": Policy(ctas_per_sm=3, stall_sweeps=1, sweeps_per_relabel=64),
     "cta4_bfsw_K2": Policy(ctas_per_sm=4, bfs_warp_min=1, local_pulses=2, sweeps_per_relabel=2),
+    "excl": Policy(exclusive=1),
+    "excl_cta3_L1_K1": Policy(exclusive=1, ctas_per_sm=3, local_pulses=1, sweeps_per_relabel=1),
+    "excl_cta4_bfsw": Policy(exclusive=1, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
+    "excl_stall": Policy(exclusive=1, stall_sweeps=1, sweeps_per_relabel=64),
 }
 
 
@@ -89,12 +93,14 @@ def test_long_paths_match_oracle(seed):
     for f in fwd + bwd:
         f[np.random.default_rng(seed).random(f.size) < 0.4] = 0
     f0, s0, t0, _ = oracle.maxflow_grid(X, Y, Z, capS, capT, fwd, bwd)
-    for pol in (None, Policy(persistent=-1), POLICIES["cta3_L2_R4"], POLICIES["cta4_no_region"]):
+    for pol in (None, Policy(persistent=-1), POLICIES["cta3_L2_R4"], POLICIES["cta4_no_region"], POLICIES["excl"],
+                POLICIES["excl_cta3_L1_K1"]):
         flow, smin, treach, _ = solve(X, Y, Z, capS, capT, fwd, bwd, pol)
         assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "cta4_R4", "bfsw_all", "bfsw8_cta4", "cta3_L2_R4"])
+@pytest.mark.parametrize("policy", ["default", "cta4_R4", "bfsw_all", "bfsw8_cta4", "cta3_L2_R4", "excl",
+                                    "excl_cta4_bfsw"])
 @pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 5) or (k[0] == 4 and k[1] < 8)])
 def test_golden_workloads(key, policy):
     c = CASES[key]
@@ -106,7 +112,7 @@ def test_golden_workloads(key, policy):
     assert sha(treach) == c["treach_sha256"]
 
 
-@pytest.mark.parametrize("policy", ["default", "bfsw8_cta4", "cta3_L2_R4"])
+@pytest.mark.parametrize("policy", ["default", "bfsw8_cta4", "cta3_L2_R4", "excl", "excl_cta4_bfsw"])
 @pytest.mark.parametrize("key", [(2, 0), (3, 0)])
 def test_full_size_workloads_with_certificate(key, policy):
     c = CASES[key]
@@ -202,7 +208,7 @@ def _face_case(X=16, Y=8, Z=8, sink_x=7, src_x=12, nlink=5):
     return X, Y, Z, capS.reshape(-1), capT.reshape(-1), [fx.reshape(-1), z, z]
 
 
-@pytest.mark.parametrize("policy", ["default", "host_loop", "cta3_L2_R4", "cta4_no_region"])
+@pytest.mark.parametrize("policy", ["default", "host_loop", "cta3_L2_R4", "cta4_no_region", "excl"])
 @pytest.mark.parametrize("sink_x,src_x", [(7, 12), (8, 3), (7, 8), (0, 15)])
 def test_seeds_on_tile_faces(sink_x, src_x, policy):
     X, Y, Z, capS, capT, fwd = _face_case(sink_x=sink_x, src_x=src_x)
@@ -212,7 +218,7 @@ def test_seeds_on_tile_faces(sink_x, src_x, policy):
     assert flow == f0 and np.array_equal(smin, s0) and np.array_equal(treach, t0)
 
 
-@pytest.mark.parametrize("policy", ["default", "host_loop", "cta3_L2_R4", "cta4_no_region"])
+@pytest.mark.parametrize("policy", ["default", "host_loop", "cta3_L2_R4", "cta4_no_region", "excl"])
 @pytest.mark.parametrize("seed", range(8))
 def test_sparse_terminals_match_oracle(seed, policy):
     """Very few t-links on a well connected grid: seeds land on tile faces and
@@ -225,7 +231,7 @@ def test_sparse_terminals_match_oracle(seed, policy):
 
 
 @pytest.mark.parametrize("policy", ["default", "host_loop", "no_region", "cta3_L2_R4", "cta4_no_region",
-                                    "bfsw_all"])
+                                    "bfsw_all", "excl", "excl_cta3_L1_K1"])
 @pytest.mark.parametrize("axis,n", [(0, 2), (0, 9), (0, 16), (0, 40), (1, 17), (2, 24), (0, 64)])
 def test_chain_through_every_voxel(axis, n, policy):
     """A 1-D chain with the source at one end and the sink at the other: the
@@ -308,7 +314,8 @@ def test_learned_scheduler_is_exact(key, learned):
             _random_scheduler_weights(weights)
         for pol in (Policy(learned=learned), Policy(learned=learned, ctas_per_sm=3, local_pulses=2, region_relabels=4,
                                                     sweeps_per_relabel=4),
-                    Policy(learned=learned, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8)):
+                    Policy(learned=learned, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
+                    Policy(learned=learned, exclusive=1, ctas_per_sm=3)):
             flow, smin, treach, st = solve(v.X, v.Y, v.Z, v.capS, v.capT, v.n, None, pol)
             assert flow == c["flow"] and sha(smin) == c["smin_sha256"] and sha(treach) == c["treach_sha256"]
 
