@@ -754,9 +754,9 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   CGC_CUDA(cudaMemcpyAsync((void*)d.tpar, tp.data(), tp.size(), cudaMemcpyHostToDevice, p->stream));
   CGC_CUDA(cudaMemcpyAsync((void*)d.geo, p->geo.data(), p->geo.size() * sizeof(InstGeo), cudaMemcpyHostToDevice, p->stream));
   p->voff.resize(count);
-  for (int i = 0; i < count; ++i) {
+  for (int i = 0; i < count; ++i) {  // offsets of multiples of 4: 16-byte aligned plane rows
     p->voff[i] = p->sumN;
-    p->sumN += (int64_t)p->geo[i].X * p->geo[i].Y * p->geo[i].Z;
+    p->sumN += ((int64_t)p->geo[i].X * p->geo[i].Y * p->geo[i].Z + 3) & ~(int64_t)3;
   }
   p->host_in.assign(8 * (size_t)count, nullptr);
   CGC_CUDA(cudaMallocHost(&p->pinned_cnt, 64 * 4));

@@ -410,23 +410,56 @@ __device__ __forceinline__ void put_tile4(const DevPool& P, const int t, const i
   const int ex[3] = {G.X, G.Y, G.Z};
   const int64_t st[3] = {1, (int64_t)G.X, (int64_t)G.X * G.Y};
   const int co[3] = {0, y, z};  // x is per voxel
-  // loads (all independent)
+  // loads (all independent).  When X is a multiple of 4, a row's four voxels
+  // start on a multiple of 4, so with 16-byte aligned planes each plane row is
+  // one int4 load (the -x neighbour of the first voxel is one more scalar);
+  // otherwise one scalar load per voxel and plane.  The choice is uniform
+  // over the block (one instance per tile).
   int s[4], c[4], fv[3][4], bv[3][4], fm[3][4], bm[3][4];
   bool ok[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    ok[k] = row && x0 + k < G.X;
-    const int64_t v = ok[k] ? vrow + k : vrow;
-    s[k] = cs[v];
-    c[k] = ct[v];
+  for (int k = 0; k < 4; ++k) ok[k] = row && x0 + k < G.X;
+  uintptr_t align = reinterpret_cast<uintptr_t>(cs) | reinterpret_cast<uintptr_t>(ct);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) align |= reinterpret_cast<uintptr_t>(fp[a]) | reinterpret_cast<uintptr_t>(bp[a]);
+  if ((G.X & 3) == 0 && (align & 15) == 0) {
+    auto ld4 = [](int (&o)[4], const int32_t* p) {
+      const int4 w = __ldg(reinterpret_cast<const int4*>(p));
+      o[0] = w.x; o[1] = w.y; o[2] = w.z; o[3] = w.w;
+    };
+    ld4(s, cs + vrow);
+    ld4(c, ct + vrow);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const int cc = a == 0 ? x0 + k : co[a];
-      const int64_t vm = cc > 0 && ok[k] ? v - st[a] : v;
-      fv[a][k] = fp[a][v];
-      bv[a][k] = bp[a][v];
-      fm[a][k] = fp[a][vm];
-      bm[a][k] = bp[a][vm];
+      ld4(fv[a], fp[a] + vrow);
+      ld4(bv[a], bp[a] + vrow);
+    }
+    const int64_t vx = row && x0 > 0 ? vrow - 1 : vrow;  // -x neighbour of the first voxel
+    fm[0][0] = __ldg(fp[0] + vx);
+    bm[0][0] = __ldg(bp[0] + vx);
+#pragma unroll
+    for (int k = 1; k < 4; ++k) { fm[0][k] = fv[0][k - 1]; bm[0][k] = bv[0][k - 1]; }
+#pragma unroll
+    for (int a = 1; a < 3; ++a) {
+      const int64_t vm = row && co[a] > 0 ? vrow - st[a] : vrow;
+      ld4(fm[a], fp[a] + vm);
+      ld4(bm[a], bp[a] + vm);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t v = ok[k] ? vrow + k : vrow;
+      s[k] = cs[v];
+      c[k] = ct[v];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int cc = a == 0 ? x0 + k : co[a];
+        const int64_t vm = cc > 0 && ok[k] ? v - st[a] : v;
+        fv[a][k] = fp[a][v];
+        bv[a][k] = bp[a][v];
+        fm[a][k] = fp[a][vm];
+        bm[a][k] = bp[a][vm];
+      }
     }
   }
   int r[6][4];
