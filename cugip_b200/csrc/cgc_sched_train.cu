@@ -6,9 +6,11 @@
 // to the sink during the relabel cycle") and a budget logit (sigmoid trained
 // with squared error against the last productive pulse of the tile's first
 // visit -- the last pulse that moved flow out of the tile or into the sink).
-// Training runs forward and backward passes in FP32 with the weights and the
-// activations rounded to BF16 in the forward pass, as inference sees them,
-// and updates FP32 master weights with Adam.
+// The forward pass runs on the tensor cores with the routine of the solve's
+// scheduler stage (BF16 weights and activations, FP32 accumulation), so the
+// network is trained on exactly the numbers inference computes; the backward
+// passes run in FP32 on the CUDA cores (the gradients are not BF16 values),
+// and Adam updates FP32 master weights.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -128,25 +130,57 @@ __device__ __forceinline__ int nb_index(int p, int D, int k, bool neg) {
   return g * D3 + nx + D * (ny + D * nz);
 }
 
+// Training forward of one convolution layer on the tensor cores: conv_rows16,
+// the routine of the solve's scheduler stage, on stacks of D^3 grids, so the
+// trained network sees exactly the inference numerics.  Writes the ReLU'd BF16
+// output (the next layer's input, may be null) and its float copy (kept for
+// the backward pass).
+__global__ void __launch_bounds__(256) k_train_conv_fwd(GridSpace sp, const uint32_t* __restrict__ in,
+                                                        const uint2* __restrict__ wf, uint32_t* out16, float* out32) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int T = sp.count(), nchunks = (T + 15) >> 4;
+  for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nchunks; c += gridDim.x * (blockDim.x >> 5)) {
+    const int ta = (c << 4) + g, tb = ta + 8;
+    const bool va = ta < T, vb = tb < T;
+    const GridCoord ca = sp.coord(va ? ta : 0), cb = sp.coord(vb ? tb : 0);
+    float acc[2][4];
+    conv_rows16(in, wf, [&](int row, int k) {
+      return row < 8 ? (va ? sp.tap(ca, k) : -1) : (vb ? sp.tap(cb, k) : -1);
+    }, acc);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float o[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) o[i] = __bfloat162float(__float2bfloat16(fmaxf(acc[h][i], 0.f)));
+      const int ch = 8 * h + 2 * q;
+      if (va) {
+        if (out16) out16[(int64_t)ta * 8 + 4 * h + q] = pack_bf16x2(o[0], o[1]);
+        out32[(int64_t)ta * SCHED_C + ch] = o[0];
+        out32[(int64_t)ta * SCHED_C + ch + 1] = o[1];
+      }
+      if (vb) {
+        if (out16) out16[(int64_t)tb * 8 + 4 * h + q] = pack_bf16x2(o[2], o[3]);
+        out32[(int64_t)tb * SCHED_C + ch] = o[2];
+        out32[(int64_t)tb * SCHED_C + ch + 1] = o[3];
+      }
+    }
+  }
+}
+
+// B fragments (fragment_order's layout) of the BF16-rounded master weights.
+__global__ void k_frag_from_f32(const float* __restrict__ wr, uint2* __restrict__ wf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // (layer, tap, half, lane)
+  if (i >= 3 * SCHED_FRAG) return;
+  const int lane = i & 31, h = (i >> 5) & 1, k = (i >> 6) % SCHED_TAPS, l = (i >> 6) / SCHED_TAPS;
+  const int g = lane >> 2, q = lane & 3, co = 8 * h + g;
+  const float* w = wr + (size_t)l * SCHED_WCONV + co;
+  wf[i] = make_uint2(pack_bf16x2(w[(k * SCHED_C + 2 * q) * SCHED_C], w[(k * SCHED_C + 2 * q + 1) * SCHED_C]),
+                     pack_bf16x2(w[(k * SCHED_C + 2 * q + 8) * SCHED_C], w[(k * SCHED_C + 2 * q + 9) * SCHED_C]));
+}
+
 __global__ void k_feat_to_f32(const __nv_bfloat16* in, float* out, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = __bfloat162float(in[i]);
-}
-
-// out[p][co] = bf16(relu(sum_k sum_ci X[nb(p,k)][ci] * W[k][ci][co]))
-__global__ void k_conv_fwd(const float* X, const float* W, float* out, int NP, int D) {
-  const int p = blockIdx.x * 16 + (threadIdx.x >> 4), co = threadIdx.x & 15;
-  if (p >= NP) return;
-  float acc = 0.f;
-  for (int k = 0; k < SCHED_TAPS; ++k) {
-    const int q = nb_index(p, D, k, false);
-    if (q < 0) continue;
-    const float* x = X + (int64_t)q * SCHED_C;
-    const float* w = W + (k * SCHED_C) * SCHED_C + co;
-#pragma unroll
-    for (int ci = 0; ci < SCHED_C; ++ci) acc = fmaf(x[ci], w[ci * SCHED_C], acc);
-  }
-  out[(int64_t)p * SCHED_C + co] = bf16_round(fmaxf(acc, 0.f));
 }
 
 // head, loss and the gradient entering the last activation
@@ -256,8 +290,12 @@ struct Trainer {
   int64_t steps = 0;
   float *w = nullptr, *wr = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   float *X = nullptr, *A[3] = {nullptr, nullptr, nullptr}, *dA = nullptr, *dB = nullptr, *stat = nullptr;
+  uint32_t* A16[2] = {nullptr, nullptr};  // BF16 copies of layers 0 and 1 (the tensor-core inputs)
+  uint2* wf = nullptr;                    // weights in mma fragment order
   ~Trainer() {
     for (float* q : {w, wr, g, m, v, X, A[0], A[1], A[2], dA, dB, stat})
+      if (q) cudaFree(q);
+    for (void* q : {(void*)A16[0], (void*)A16[1], (void*)wf})
       if (q) cudaFree(q);
   }
 };
@@ -271,10 +309,13 @@ static int trainer_forward_backward(Trainer& tr, int grids, const uint16_t* feat
   if (backward) CGC_CUDA(cudaMemset(tr.g, 0, tr.nparam * sizeof(float)));
   k_feat_to_f32<<<1024, 256>>>((const __nv_bfloat16*)feat, tr.X, (int64_t)NP * SCHED_C);
   const int blocks = (NP + 15) / 16;
-  const float* in = tr.X;
+  k_frag_from_f32<<<(3 * SCHED_FRAG + 255) / 256, 256>>>(tr.wr, tr.wf);
+  const GridSpace sp{grids, tr.D};
+  const unsigned cblocks = (unsigned)std::min((NP + 127) / 128, 8192);
+  const uint32_t* in16 = reinterpret_cast<const uint32_t*>(feat);
   for (int l = 0; l < 3; ++l) {
-    k_conv_fwd<<<blocks, 256>>>(in, tr.wr + l * SCHED_WCONV, tr.A[l], NP, tr.D);
-    in = tr.A[l];
+    k_train_conv_fwd<<<cblocks, 256>>>(sp, in16, tr.wf + (size_t)l * SCHED_FRAG, l < 2 ? tr.A16[l] : nullptr, tr.A[l]);
+    if (l < 2) in16 = tr.A16[l];
   }
   const float* wh = tr.wr + 3 * SCHED_WCONV;
   k_head_loss<<<(NP + 255) / 256, 256>>>(tr.A[2], wh, yp, yb, mask, inv_n, tr.dA,
@@ -402,6 +443,9 @@ int cgc_trainer_create(int32_t max_grids, int32_t D, uint64_t seed, cgc_trainer*
   for (float** q : {&tr.X, &tr.A[0], &tr.A[1], &tr.A[2], &tr.dA, &tr.dB})
     if (e == cudaSuccess) e = cudaMalloc(q, act * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&tr.stat, 4 * sizeof(float));
+  for (uint32_t** q : {&tr.A16[0], &tr.A16[1]})
+    if (e == cudaSuccess) e = cudaMalloc(q, act * 2);
+  if (e == cudaSuccess) e = cudaMalloc(&tr.wf, (size_t)3 * cgc::SCHED_FRAG * sizeof(uint2));
   if (e != cudaSuccess) { delete T; return cgc::fail(CGC_ERR_OOM, "cgc_trainer_create: device allocation"); }
   // He-uniform initialisation of the convolutions, small head
   std::mt19937_64 rng(seed);

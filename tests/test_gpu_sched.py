@@ -84,3 +84,58 @@ def test_tensor_core_cnn_matches_fp32_reference(grids, D, seed):
     z = logits.cpu().numpy().reshape(T, 2)
     assert np.array_equal(z[:, 0], np.full(T, head[32], np.float32))
     assert np.array_equal(z[:, 1], np.full(T, head[33], np.float32))
+
+
+def test_trainer_learns_a_synthetic_target_and_inference_agrees():
+    """cgc_trainer_step (tensor-core forward, FP32 backward, Adam) on a learnable
+    target -- priority = (feature 0 of the tile > 0.5), budget = feature 1 --
+    lowers the loss, and the trained weights run through the solve's inference
+    kernels (cgc_scheduler_infer) reproduce the priorities on the active tiles."""
+    import torch
+    lib = _lib.load()
+    D, grids, steps = 8, 8, 300
+    T = D ** 3
+    rng = np.random.default_rng(5)
+    dev = torch.device("cuda", 0)
+
+    def batch():
+        f = np.zeros((grids, T, 16), np.float32)
+        act = rng.random((grids, T)) < 0.4
+        f[..., :10] = rng.random((grids, T, 10)) * act[..., None]
+        f = torch.from_numpy(f).to(torch.bfloat16)
+        fv = f.float().numpy()
+        prio = ((fv[..., 0] > 0.5) & act).astype(np.float32)
+        bud = np.clip(fv[..., 1], 0, 1).astype(np.float32)
+        return f.view(torch.int16).to(dev).contiguous(), torch.from_numpy(prio).to(dev), \
+            torch.from_numpy(bud).to(dev), torch.from_numpy(act.astype(np.float32)).to(dev), act, fv
+
+    h = C.c_void_p()
+    _lib.check(lib.cgc_trainer_create(grids, D, 11, C.byref(h)))
+    try:
+        ev = batch()
+        loss0, acc0 = C.c_float(), C.c_float()
+        _lib.check(lib.cgc_trainer_eval(h, grids, ev[0].data_ptr(), ev[1].data_ptr(), ev[2].data_ptr(), ev[3].data_ptr(),
+                                        float(ev[4].sum()), C.byref(loss0), C.byref(acc0)))
+        loss = C.c_float()
+        for _ in range(steps):
+            b = batch()
+            _lib.check(lib.cgc_trainer_step(h, grids, b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr(), b[3].data_ptr(),
+                                            float(b[4].sum()), 3e-3, C.byref(loss)))
+        loss1, acc1 = C.c_float(), C.c_float()
+        _lib.check(lib.cgc_trainer_eval(h, grids, ev[0].data_ptr(), ev[1].data_ptr(), ev[2].data_ptr(), ev[3].data_ptr(),
+                                        float(ev[4].sum()), C.byref(loss1), C.byref(acc1)))
+        assert loss1.value < 0.6 * loss0.value, (loss0.value, loss1.value)
+        assert acc1.value > 0.85, acc1.value
+        conv = np.zeros(3 * 27 * 256, np.uint16)
+        head = np.zeros(34, np.float32)
+        _lib.check(lib.cgc_trainer_weights(h, conv.ctypes.data, head.ctypes.data))
+    finally:
+        lib.cgc_trainer_destroy(h)
+    _lib.check(lib.cgc_scheduler_load(conv.ctypes.data, head.ctypes.data))
+    budget = torch.zeros(grids * T, dtype=torch.uint8, device=dev)
+    prio = torch.zeros(grids * T, dtype=torch.uint8, device=dev)
+    _lib.check(lib.cgc_scheduler_infer(grids, D, ev[0].data_ptr(), budget.data_ptr(), prio.data_ptr(), None, None))
+    act = ev[4].reshape(-1)
+    want = (ev[5][..., 0] > 0.5).reshape(-1)
+    got = prio.cpu().numpy().astype(bool)
+    assert (got[act] == want[act]).mean() > 0.85
