@@ -418,9 +418,12 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     const int cycle = (int)relabels - 1;
     const bool tracing = prm.trace_cycles > cycle;
     if (tracing) traced = cycle + 1;
-    // The scheduler only pays off while active tiles outnumber the CTAs: with
-    // fewer, a sweep lasts one tile visit whatever the order or budgets.
-    const bool learned = prm.learned && nact > 2 * G;
+    // Priorities (deferral) only pay off while active tiles outnumber the
+    // CTAs: with fewer, a sweep lasts one tile visit whatever the order.
+    // Budgets can still shorten that visit, so learned = 3 runs the stage in
+    // every cycle.
+    const bool throughput = nact > 2 * G;
+    const bool learned = prm.learned && (throughput || prm.learned == 3);
     if (learned || tracing) {
       if (!sched_stage(P, prm, cycle, learned, tracing, S.sched)) return;
       lap(ns_sched);
@@ -442,7 +445,7 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
       ex.sink_tiles = P.cnt + C_SINKT0 + (int)(s % 3);
       // the learned scheduler defers low-priority tiles during the first half
       // of the cycle; every active tile is swept in the second half
-      const bool may_defer = learned && prm.learned == 1 && j < prm.K;
+      const bool may_defer = learned && throughput && (prm.learned == 1 || prm.learned == 3) && j < prm.K;
       // Parity sweeps: sweep s uses stamp id s + 1; a visited tile queues the
       // tiles it pushed into for sweep s + 1 and itself, of the same parity,
       // for sweep s + 2.  Exclusive sweeps: every queued tile runs unless it
@@ -873,7 +876,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
     r.bfs_warp_min = o->bfs_warp_min > 0 ? o->bfs_warp_min : 0;
     r.exclusive = o->exclusive > 0 ? 1 : 0;
-    r.learned = o->learned == 2 ? 2 : (o->learned > 0 ? 1 : 0);
+    r.learned = (o->learned == 2 || o->learned == 3) ? o->learned : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
   return r;
