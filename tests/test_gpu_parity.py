@@ -297,7 +297,7 @@ def _random_scheduler_weights(seed):
     _lib.check(lib.cgc_scheduler_load(conv.ctypes.data, head.ctypes.data))
 
 
-@pytest.mark.parametrize("learned", [1, 2])
+@pytest.mark.parametrize("learned", [1, 2, 3])
 @pytest.mark.parametrize("key", [(1, 0), (4, 1), (2, 0)])
 def test_learned_scheduler_is_exact(key, learned):
     """Budgets and priorities only reorder pushes and relabels: flow and both
