@@ -76,16 +76,22 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def learned_report(workloads=(1, 3)) -> dict:
-    """The learned scheduler against the same fixed schedule without it, on the
-    64^3 two-sphere and 512x512x128 tube workloads: kernel time, exact global
-    relabels (saved = plain - learned) and bit-identity of the flow and of
-    both cut sets."""
+LEARNED_MODES = {1: "budgets + priorities in throughput-bound cycles", 2: "budgets only, throughput-bound cycles",
+                 3: "budgets in every cycle + priorities in throughput-bound cycles"}
+
+
+def learned_report(workloads=(1, 2, 3)) -> dict:
+    """The learned scheduler (each mode) against the same fixed schedule without
+    it, on the 64^3 two-sphere, 256^3 forty-sphere and 512x512x128 tube
+    workloads: kernel time, time in the scheduler stage, sweeps, exact global
+    relabels (saved = plain - learned), tile visits, pulses and bit-identity of
+    the flow and of both cut sets."""
     import hashlib
-    import numpy as np
     import torch
     from cugip_b200 import volume
     from cugip_b200.graph_cut import SINK, SOURCE, GridGraph, Policy
+    base = dict(local_pulses=4, region_relabels=2, sweeps_per_relabel=8, ctas_per_sm=3)
+    keep = ("kernel_ms", "sched_ms", "sweeps", "global_relabels", "tiles_swept", "pulses")
     out = {}
     for w in workloads:
         v = volume.workload(w)
@@ -93,9 +99,8 @@ def learned_report(workloads=(1, 3)) -> dict:
         g = GridGraph(v.X, v.Y, v.Z)
         res = {}
         try:
-            for name, pol in (("plain", Policy(local_pulses=4, region_relabels=2, sweeps_per_relabel=8, ctas_per_sm=3)),
-                              ("learned", Policy(local_pulses=4, region_relabels=2, sweeps_per_relabel=8, ctas_per_sm=3,
-                                                 learned=1))):
+            for mode in (0, 1, 2, 3):
+                pol = Policy(learned=mode, **base)
                 runs = []
                 for _ in range(3):
                     g.set_tweights_device(d[0].data_ptr(), d[1].data_ptr())
@@ -105,13 +110,17 @@ def learned_report(workloads=(1, 3)) -> dict:
                     runs.append(g.stats())
                 cuts = [hashlib.sha256(g.fill_segments(mask=1, which=k).tobytes()).hexdigest() for k in (SOURCE, SINK)]
                 best = min(runs, key=lambda s: s["kernel_ms"])
-                res[name] = (flow, cuts, best["kernel_ms"], int(best["global_relabels"]))
+                res[mode] = (flow, cuts, {k: best[k] for k in keep})
         finally:
             g.close()
-        (fp, cp, mp, rp), (fl, cl, ml, rl) = res["plain"], res["learned"]
-        out[f"workload{w}"] = {"voxels": v.N, "plain_ms": mp, "learned_ms": ml, "speedup": mp / ml,
-                               "relabels_plain": rp, "relabels_learned": rl, "relabels_saved": rp - rl,
-                               "bit_identical": fp == fl and cp == cl}
+        plain = res[0]
+        rep = {"voxels": v.N, "schedule": repr(Policy(**base)), "plain": plain[2]}
+        for mode in (1, 2, 3):
+            fl, cu, st = res[mode]
+            rep[f"learned{mode}"] = dict(st, mode=LEARNED_MODES[mode], speedup=plain[2]["kernel_ms"] / st["kernel_ms"],
+                                         relabels_saved=plain[2]["global_relabels"] - st["global_relabels"],
+                                         bit_identical=fl == plain[0] and cu == plain[1])
+        out[f"workload{w}"] = rep
     return out
 
 
