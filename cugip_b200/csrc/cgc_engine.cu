@@ -421,7 +421,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     // Priorities (deferral) only pay off while active tiles outnumber the
     // CTAs: with fewer, a sweep lasts one tile visit whatever the order.
     // Budgets can still shorten that visit, so learned = 3 runs the stage in
-    // every cycle.
+    // every cycle, with each tile's budget capped at the schedule's L (a
+    // budget may only end a visit early).
     const bool throughput = nact > 2 * G;
     const bool learned = prm.learned && (throughput || prm.learned == 3);
     if (learned || tracing) {
@@ -476,7 +477,8 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
             return;
           }
         }
-        const int L = learned ? (int)__ldcg(P.sbudget + t) : prm.L;
+        const int L = !learned ? prm.L
+                      : prm.learned == 3 ? min((int)__ldcg(P.sbudget + t), prm.L) : (int)__ldcg(P.sbudget + t);
         sweep_tile<true>(P, t, L, prm.R, S.sw, (uint32_t)(s + 2), sl[(s + 1) & 3], sc + ((s + 1) & 3), id_self,
                          list_self, cnt_self, ex, stamp_q);
       });

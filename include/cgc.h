@@ -74,9 +74,9 @@ typedef struct cgc_options {
   int32_t region_relabels;    /* region-relabel rounds per tile visit (default 2, -1 = none) */
   int32_t stall_sweeps;       /* persistent: relabel early after this many sweep pairs without sink flow (0 = never) */
   int32_t ctas_per_sm;        /* persistent: 2 (default, 64 registers), 3 (40) or 4 (32 registers) */
-  int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only,
-                                 3 = budgets in every relabel cycle + priorities; 1 and 2 run the scheduler only
-                                 in cycles with more active tiles than twice the CTAs */
+  int32_t learned;            /* persistent: learned scheduler, 1 = budgets + priorities, 2 = budgets only
+                                 (both only in cycles with more active tiles than twice the CTAs), 3 = budgets
+                                 capped at local_pulses in every cycle + priorities where 1 uses them */
   int32_t trace_cycles;       /* persistent: record scheduling traces of the first trace_cycles relabel cycles */
   int32_t bfs_warp_min;       /* persistent, 3 or 4 CTAs/SM: BFS rounds with at least this many tiles per CTA
                                  visit a tile with one warp (0 = never, the default) */
