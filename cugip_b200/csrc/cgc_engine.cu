@@ -240,20 +240,31 @@ __device__ __forceinline__ int ld_cnt(const int32_t* p) { return *(volatile cons
 // Learned-scheduler stage at the start of a relabel cycle: the features of
 // every tile (zero for inactive ones; recorded when tracing), then the three
 // convolution layers on the tensor cores, the last one with the head (budgets
-// and priorities).  Four grid barriers.  Returns false when a barrier failed.
+// and priorities).  The active tiles are the entries of the cycle's first
+// lists (la: na entries, lb: nb).  Four grid barriers.  Returns false when a
+// barrier failed.
 __device__ __forceinline__ bool sched_stage(const DevPool& P, const SolveParams& prm, int cycle, bool learned,
-                                            bool tracing, SchedShared& sh) {
-  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+                                            bool tracing, const int32_t* la, int na, const int32_t* lb, int nb) {
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   const int gw = b * (blockDim.x >> 5) + (tid >> 5), nw = G * (blockDim.x >> 5);
-  for (int t = gw; t < P.T; t += nw) {
+  // zeros for the inactive tiles, a thread per tile
+  for (int t = b * blockDim.x + tid; t < P.T; t += G * blockDim.x) {
     const int64_t r = (int64_t)cycle * P.T + t;  // trace row
-    if (__ldcg(P.act + t)) {
-      sched_features_warp(P, t, P.sfeat, tracing ? P.tfeat + r * SCHED_C : nullptr);
-    } else if (lane < 8) {
-      reinterpret_cast<uint32_t*>(P.sfeat)[(int64_t)t * 8 + lane] = 0u;
-      if (tracing) reinterpret_cast<uint32_t*>(P.tfeat)[r * 8 + lane] = 0u;
+    if (tracing) { P.tpulses[r] = 0; P.tsink[r] = 0; }
+    if (__ldcg(P.act + t)) continue;
+    uint4* f = reinterpret_cast<uint4*>(P.sfeat + (int64_t)t * SCHED_C);
+    f[0] = make_uint4(0, 0, 0, 0);
+    f[1] = make_uint4(0, 0, 0, 0);
+    if (tracing) {
+      uint4* tf = reinterpret_cast<uint4*>(P.tfeat + r * SCHED_C);
+      tf[0] = make_uint4(0, 0, 0, 0);
+      tf[1] = make_uint4(0, 0, 0, 0);
     }
-    if (tracing && lane == 0) { P.tpulses[r] = 0; P.tsink[r] = 0; }
+  }
+  // features of the active tiles, a warp per list entry
+  for (int i = gw; i < na + nb; i += nw) {
+    const int t = __ldcg(i < na ? la + i : lb + (i - na));
+    sched_features_warp(P, t, P.sfeat, tracing ? P.tfeat + ((int64_t)cycle * P.T + t) * SCHED_C : nullptr);
   }
   if (!grid_sync(P, prm.limit_ns)) return false;
   if (!learned) return true;
@@ -426,7 +437,9 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     const bool throughput = nact > 2 * G;
     const bool learned = prm.learned && (throughput || prm.learned == 3);
     if (learned || tracing) {
-      if (!sched_stage(P, prm, cycle, learned, tracing, S.sched)) return;
+      if (!sched_stage(P, prm, cycle, learned, tracing, sl[s & 3], ld_cnt(sc + (s & 3)), sl[(s + 1) & 3],
+                       prm.exclusive ? 0 : ld_cnt(sc + ((s + 1) & 3))))
+        return;
       lap(ns_sched);
     }
     // ------------------------------------------------ sweeps

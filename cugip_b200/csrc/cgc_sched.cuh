@@ -130,9 +130,9 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 }
 
 // acc[h][0..1]: row g, channels 8h + 2q, +1; acc[h][2..3]: row g + 8.  `tap(row, k)`
-// gives the neighbour tile of row 0..15 at tap k (-1: none); `in` holds 8
-// words (16 BF16 channels) per tile.  Taps whose 16 rows are all zero add
-// exactly nothing and are skipped.
+// gives the neighbour tile of row 0..15 at tap k (-1: none, a zero row); `in`
+// holds 8 words (16 BF16 channels) per tile.  The loop has no warp vote, so
+// the loads of consecutive taps are in flight together.
 template <typename Tap>
 __device__ __forceinline__ void conv_rows16(const uint32_t* __restrict__ in, const uint2* __restrict__ wf, Tap&& tap,
                                             float (&acc)[2][4]) {
@@ -141,13 +141,13 @@ __device__ __forceinline__ void conv_rows16(const uint32_t* __restrict__ in, con
   for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc[h][i] = 0.f;
+#pragma unroll 3
   for (int k = 0; k < SCHED_TAPS; ++k) {
     const int na = tap(g, k), nb = tap(g + 8, k);
     const uint32_t a0 = na >= 0 ? __ldcg(in + (int64_t)na * 8 + q) : 0u;
     const uint32_t a1 = nb >= 0 ? __ldcg(in + (int64_t)nb * 8 + q) : 0u;
     const uint32_t a2 = na >= 0 ? __ldcg(in + (int64_t)na * 8 + 4 + q) : 0u;
     const uint32_t a3 = nb >= 0 ? __ldcg(in + (int64_t)nb * 8 + 4 + q) : 0u;
-    if (!__any_sync(0xffffffffu, (a0 | a1 | a2 | a3) != 0u)) continue;
     const uint2 w0 = __ldg(wf + (k * 2) * 32 + lane), w1 = __ldg(wf + (k * 2 + 1) * 32 + lane);
     mma_bf16_16816(acc[0], a0, a1, a2, a3, w0.x, w0.y);
     mma_bf16_16816(acc[1], a0, a1, a2, a3, w1.x, w1.y);
