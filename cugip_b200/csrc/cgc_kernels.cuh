@@ -410,11 +410,11 @@ __device__ __forceinline__ void put_tile4(const DevPool& P, const int t, const i
   const int ex[3] = {G.X, G.Y, G.Z};
   const int64_t st[3] = {1, (int64_t)G.X, (int64_t)G.X * G.Y};
   const int co[3] = {0, y, z};  // x is per voxel
-  // loads (all independent).  When X is a multiple of 4, a row's four voxels
-  // start on a multiple of 4, so with 16-byte aligned planes each plane row is
-  // one int4 load (the -x neighbour of the first voxel is one more scalar);
-  // otherwise one scalar load per voxel and plane.  The choice is uniform
-  // over the block (one instance per tile).
+  // loads (all independent).  With 16-byte aligned planes (the choice is
+  // uniform over the block: one instance per tile), each plane row of the
+  // thread's four voxels v..v+3 is read as the one or two aligned int4 that
+  // cover it (load_row4); a row that would reach past the plane's end falls
+  // back to scalar loads.  Otherwise one scalar load per voxel and plane.
   int s[4], c[4], fv[3][4], bv[3][4], fm[3][4], bm[3][4];
   bool ok[4];
 #pragma unroll
@@ -422,17 +422,29 @@ __device__ __forceinline__ void put_tile4(const DevPool& P, const int t, const i
   uintptr_t align = reinterpret_cast<uintptr_t>(cs) | reinterpret_cast<uintptr_t>(ct);
 #pragma unroll
   for (int a = 0; a < 3; ++a) align |= reinterpret_cast<uintptr_t>(fp[a]) | reinterpret_cast<uintptr_t>(bp[a]);
-  if ((G.X & 3) == 0 && (align & 15) == 0) {
-    auto ld4 = [](int (&o)[4], const int32_t* p) {
-      const int4 w = __ldg(reinterpret_cast<const int4*>(p));
-      o[0] = w.x; o[1] = w.y; o[2] = w.z; o[3] = w.w;
+  const int64_t N = (int64_t)G.X * G.Y * G.Z;
+  if ((align & 15) == 0) {
+    // p[v .. v+3] from aligned int4 loads (p 16-byte aligned, 0 <= v < N)
+    auto load_row4 = [N](int (&o)[4], const int32_t* p, int64_t v) {
+      const int m = (int)(v & 3);
+      const int64_t a = v - m;
+      if (a + (m ? 8 : 4) <= N) {
+        const int4 A = __ldg(reinterpret_cast<const int4*>(p + a));
+        const int4 B = m ? __ldg(reinterpret_cast<const int4*>(p + a + 4)) : A;
+        const int w[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = m == 0 ? w[k] : m == 1 ? w[k + 1] : m == 2 ? w[k + 2] : w[k + 3];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = p[v + k < N ? v + k : v];
+      }
     };
-    ld4(s, cs + vrow);
-    ld4(c, ct + vrow);
+    load_row4(s, cs, vrow);
+    load_row4(c, ct, vrow);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      ld4(fv[a], fp[a] + vrow);
-      ld4(bv[a], bp[a] + vrow);
+      load_row4(fv[a], fp[a], vrow);
+      load_row4(bv[a], bp[a], vrow);
     }
     const int64_t vx = row && x0 > 0 ? vrow - 1 : vrow;  // -x neighbour of the first voxel
     fm[0][0] = __ldg(fp[0] + vx);
@@ -442,8 +454,8 @@ __device__ __forceinline__ void put_tile4(const DevPool& P, const int t, const i
 #pragma unroll
     for (int a = 1; a < 3; ++a) {
       const int64_t vm = row && co[a] > 0 ? vrow - st[a] : vrow;
-      ld4(fm[a], fp[a] + vm);
-      ld4(bm[a], bp[a] + vm);
+      load_row4(fm[a], fp[a], vm);
+      load_row4(bm[a], bp[a], vm);
     }
   } else {
 #pragma unroll
