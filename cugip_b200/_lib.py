@@ -37,7 +37,8 @@ class Options(C.Structure):
                 ("wait_limit_us", C.c_int32), ("max_sweeps", C.c_int32), ("persistent", C.c_int32),
                 ("region_relabels", C.c_int32), ("stall_sweeps", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("learned", C.c_int32), ("trace_cycles", C.c_int32),
-                ("bfs_warp_min", C.c_int32), ("exclusive", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("bfs_warp_min", C.c_int32), ("exclusive", C.c_int32), ("relabel", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Stats(C.Structure):
@@ -45,7 +46,8 @@ class Stats(C.Structure):
                 ("bfs_rounds", C.c_int64), ("tiles_swept", C.c_int64), ("tiles_relabelled", C.c_int64),
                 ("pulses", C.c_int64), ("solve_ms", C.c_double), ("kernel_ms", C.c_double),
                 ("launches", C.c_int64), ("bfs_ms", C.c_double), ("sweep_ms", C.c_double),
-                ("reach_ms", C.c_double), ("sched_ms", C.c_double), ("reserved", C.c_int64 * 2)]
+                ("reach_ms", C.c_double), ("sched_ms", C.c_double), ("tiles_checked", C.c_int64),
+                ("reserved", C.c_int64 * 1)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -149,7 +151,7 @@ def check(rc: int) -> None:
 
 OPTION_FIELDS = ("local_pulses", "sweeps_per_relabel", "wait_limit_us", "max_sweeps", "persistent",
                  "region_relabels", "stall_sweeps", "ctas_per_sm", "learned", "trace_cycles", "bfs_warp_min",
-                 "exclusive")
+                 "exclusive", "relabel")
 
 
 def options(**fields) -> Options:

@@ -46,17 +46,23 @@ void load_cache_locked() {
   if (!path) return;
   FILE* f = std::fopen(path, "r");
   if (!f) return;
-  // line: size class (2), L R K ctas stall learned bfs_warp_min, milliseconds
+  // line: size class (2), L R K ctas stall learned bfs_warp_min exclusive
+  // relabel, milliseconds (lines without exclusive and relabel are read too)
   char line[256];
   while (std::fgets(line, sizeof line, f)) {
-    int ib, vb, L, R, K, cta, st, lr, bw;
+    int ib, vb, L, R, K, cta, st, lr, bw, ex = 0, rl = 0;
     double ms;
-    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &lr, &bw, &ms) != 10) continue;
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &lr, &bw, &ex, &rl,
+                    &ms) != 12 &&
+        std::sscanf(line, "%d %d %d %d %d %d %d %d %d %lf", &ib, &vb, &L, &R, &K, &cta, &st, &lr, &bw, &ms) != 10)
+      continue;
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
     o.local_pulses = L; o.region_relabels = R; o.sweeps_per_relabel = K; o.ctas_per_sm = cta; o.stall_sweeps = st;
     o.learned = lr;
     o.bfs_warp_min = bw;
+    o.exclusive = ex;
+    o.relabel = rl;
     g_cache[{ib, vb}] = {o, ms};
   }
   std::fclose(f);
@@ -68,8 +74,9 @@ void store(std::pair<int, int> key, const cgc_options& o, double ms) {
   g_cache[key] = {o, ms};
   if (const char* path = std::getenv("CGC_AUTOTUNE_CACHE")) {
     if (FILE* f = std::fopen(path, "a")) {
-      std::fprintf(f, "%d %d %d %d %d %d %d %d %d %.6f\n", key.first, key.second, o.local_pulses, o.region_relabels,
-                   o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.learned, o.bfs_warp_min, ms);
+      std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d %d %.6f\n", key.first, key.second, o.local_pulses,
+                   o.region_relabels, o.sweeps_per_relabel, o.ctas_per_sm, o.stall_sweeps, o.learned, o.bfs_warp_min,
+                   o.exclusive, o.relabel, ms);
       std::fclose(f);
     }
   }

@@ -104,6 +104,7 @@ int pool_enqueue(Pool& p, const cgc_options* opts, int64_t* flows_dev, cudaStrea
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, 2 * (size_t)d.T * 4, stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_inc, 0, (size_t)d.T * 4, stream));
   k_put_all<<<d.T, 128, 0, stream>>>(d, p.d_in);
   note_launch();
   const SolveParams prm = solve_params(o);
@@ -140,6 +141,7 @@ int pool_wait(Pool& p, cudaStream_t stream) {
   p.st.bfs_rounds = (int64_t)stats[S_ROUNDS];
   p.st.tiles_swept = (int64_t)stats[S_TILES_SWEPT];
   p.st.tiles_relabelled = (int64_t)stats[S_TILES_BFS];
+  p.st.tiles_checked = (int64_t)stats[S_TILES_CHECK];
   p.st.pulses = (int64_t)stats[S_PULSES];
   p.st.bfs_ms = 1e-6 * (double)stats[S_NS_BFS];
   p.st.sweep_ms = 1e-6 * (double)stats[S_NS_SWEEP];

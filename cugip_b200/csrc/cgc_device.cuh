@@ -39,6 +39,7 @@ enum Counter {
   C_ROUNDS = 8,    // BFS rounds executed
   C_SINKT0 = 9,    // 3 slots: tiles that delivered flow to the sink in a sweep
   C_TAKE0 = 12,    // 3 slots: next list entry to hand out in a round (persistent solve)
+  C_INC = 15,      // incremental relabel: tiles with dropped voxels (the BFS rounds' first list)
   C_NCOUNTERS = 16
 };
 
@@ -46,7 +47,8 @@ enum Counter {
 enum Stat {
   S_TILES_SWEPT = 0, S_PULSES = 1, S_TILES_BFS = 2, S_SWEEPS = 3, S_RELABELS = 4, S_ROUNDS = 5,
   S_NS_BFS = 6, S_NS_SWEEP = 7, S_NS_REACH = 8, S_TRACE_N = 9, S_TRACE_CYC = 10, S_NS_SCHED = 11,
-  S_BOUND_AT = 12 /* bounds-checked build: the first index found out of range */, S_NSTATS = 13
+  S_BOUND_AT = 12 /* bounds-checked build: the first index found out of range */,
+  S_TILES_CHECK = 13 /* tile visits of the incremental relabels' invalidation passes */, S_NSTATS = 14
 };
 
 // phase trace records written by the persistent solve (two words each):
@@ -85,6 +87,8 @@ struct DevPool {
   uint16_t* tflag;      // T: BFS seed summary (TF_* bits)
   uint32_t* stamp_bfs;  // T: last BFS round the tile was queued for
   uint32_t* stamp_sw;   // 2*T: last sweep the tile was queued for (exclusive sweeps: half s&1 for sweep s)
+  uint32_t* stamp_inc;  // T: last incremental relabel that listed the tile for its BFS rounds (may be null:
+                        //    then every relabel is a full BFS)
   int32_t* lists;       // 7*T worklists: 3 for the BFS, 4 for the sweeps
   int32_t* cnt;         // C_NCOUNTERS
   unsigned long long* flow;   // ninst: flow value (int64 as two's complement)
@@ -119,6 +123,7 @@ struct SolveParams {
   uint64_t limit_ns;     // bounded barrier wait
   int bfs_warp_min = 0;  // BFS rounds with at least this many tiles per CTA run a warp per tile (0: never)
   int exclusive = 0;     // 1: exclusive sweeps (cgc_options.exclusive), 0: parity sweeps
+  int incremental = 0;   // 1: global relabels after the first of a solve are incremental (cgc_options.relabel)
 };
 
 // kernels of cgc_engine.cu launched from other translation units

@@ -345,27 +345,25 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
     acc += now - tmark;
     tmark = now;
   };
-  for (;;) {
-    // ------------------------------------------------ exact global relabel
-    if (b == 0 && tid == 0) {
-      bc[0] = bc[1] = bc[2] = 0;
-      sc[0] = sc[1] = sc[2] = sc[3] = 0;
-      P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
-      P.cnt[C_TAKE0] = P.cnt[C_TAKE0 + 1] = P.cnt[C_TAKE0 + 2] = 0;
-    }
-    round_no = 0;
-    if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);  // a warp per tile in both shapes
-    if (!grid_sync(P, prm.limit_ns)) return;
-    for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x) bfs_queue_tile(P, t0 + tid, bfs_id, bl[0], bc + 0);
-    if (!grid_sync(P, prm.limit_ns)) return;
+  // Tile rounds of one relabel pass: round 0 visits the entries of list0
+  // (count *cnt0), round k > 0 the tiles round k - 1 queued in bl[k % 3]
+  // (bc[1], bc[2] zero on entry).  inval: invalidation visits, otherwise BFS
+  // visits.  False when a grid barrier gave up.
+  auto relabel_rounds = [&](int32_t* list0, int32_t* cnt0, bool inval) -> bool {
     int k = 0;
     for (;;) {
-      int n = ld_cnt(bc + k % 3);
+      int32_t* const lst = k == 0 ? list0 : bl[k % 3];
+      int n = ld_cnt(k == 0 ? cnt0 : bc + k % 3);
       if (n == 0) break;
       if (!CGC_IN_BOUNDS(P, n, P.T + 1)) n = P.T;  // a list holds at most T entries
       if (b == 0 && tid == 0) bc[(k + 2) % 3] = 0;
-      if (BFSW && n / G >= prm.bfs_warp_min) {
+      if (inval) {
+        const uint32_t id_inc = (uint32_t)(relabels + 1);
+        for_entries(n, [&](int i) {
+          inval_tile(P, __ldcg(lst + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3, id_inc, sl[0],
+                     P.cnt + C_INC);
+        });
+      } else if (BFSW && n / G >= prm.bfs_warp_min) {
         // Throughput-bound round: a warp per tile (no block barriers, a
         // tile's relaxation costs one warp's issue slots instead of 16),
         // entries handed out like for_entries, per warp.
@@ -378,25 +376,61 @@ __device__ __forceinline__ void solve_body(const DevPool& P, const SolveParams& 
           while (i < n) {
             int nx = 0;
             if ((tid & 31) == 0) nx = atomicAdd(take, 1);
-            bfs_tile_w(P, __ldcg(bl[k % 3] + i), S.wbfs[wid], bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+            bfs_tile_w(P, __ldcg(lst + i), S.wbfs[wid], bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
             i = G * BFS_WARPS + __shfl_sync(0xffffffffu, nx, 0);
           }
         }
       } else {
         for_entries(n, [&](int i) {
-          bfs_tile(P, __ldcg(bl[k % 3] + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
+          bfs_tile(P, __ldcg(lst + i), S.bfs, bfs_id + k + 1, bl[(k + 1) % 3], bc + (k + 1) % 3);
         });
       }
       ++k;
-      if (!grid_sync(P, prm.limit_ns)) return;
+      if (!grid_sync(P, prm.limit_ns)) return false;
       record(TR_BFS_ROUND, rounds + k, n);
     }
     bfs_id += k + 1;
     rounds += k;
+    return true;
+  };
+  uint32_t c0 = 0;  // sweep stamps above c0 were written during the current cycle
+  for (;;) {
+    // ------------------------------------------------ exact global relabel
+    // The first relabel of a solve is a full BFS from the sink; later ones
+    // are incremental when the pool has the stamps for it.
+    const bool inc = prm.incremental && relabels > 0 && P.stamp_inc != nullptr;
+    if (b == 0 && tid == 0) {
+      bc[0] = bc[1] = bc[2] = 0;
+      sc[0] = sc[1] = sc[2] = sc[3] = 0;
+      P.cnt[C_SINKT0] = P.cnt[C_SINKT0 + 1] = P.cnt[C_SINKT0 + 2] = 0;
+      P.cnt[C_TAKE0] = P.cnt[C_TAKE0 + 1] = P.cnt[C_TAKE0 + 2] = 0;
+      P.cnt[C_INC] = 0;
+    }
+    round_no = 0;
+    if (!grid_sync(P, prm.limit_ns)) return;
+    if (!inc) {
+      for (int t = gw; t < P.T; t += nw) bfs_init_tile_w(P, t);  // a warp per tile in both shapes
+      if (!grid_sync(P, prm.limit_ns)) return;
+      for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x) bfs_queue_tile(P, t0 + tid, bfs_id, bl[0], bc + 0);
+      if (!grid_sync(P, prm.limit_ns)) return;
+      if (!relabel_rounds(bl[0], bc + 0, false)) return;
+    } else {
+      // invalidation from the tiles the last cycle queued, then BFS rounds
+      // from the tiles with dropped voxels (listed in sl[0], free until the
+      // sweep lists are rebuilt below)
+      for (int t0 = b * blockDim.x; t0 < P.T; t0 += G * blockDim.x)
+        inval_queue_tile(P, t0 + tid, c0, prm.exclusive != 0, bfs_id, bl[0], bc + 0);
+      if (!grid_sync(P, prm.limit_ns)) return;
+      if (!relabel_rounds(bl[0], bc + 0, true)) return;
+      if (b == 0 && tid == 0) bc[0] = bc[1] = bc[2] = 0;
+      if (!grid_sync(P, prm.limit_ns)) return;
+      if (!relabel_rounds(sl[0], P.cnt + C_INC, false)) return;
+    }
     ++relabels;
     lap(ns_bfs);
     // ------------------------------------------------ active tiles -> parity lists
     s += 2;  // fresh stamp ids for the lists built here
+    c0 = (uint32_t)s;
     for (int t0 = b * blockDim.x + (tid & ~31); t0 < P.T; t0 += G * blockDim.x) {  // warp-aggregated appends
       const int t = t0 + (tid & 31);
       const bool a = t < P.T && __ldcg(P.act + t);
@@ -725,6 +759,7 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   const int64_t o_tf = off; off += al(T * 2);
   const int64_t o_sb = off; off += al(T * 4);
   const int64_t o_ss = off; off += al(2 * T * 4);
+  const int64_t o_si = off; off += al(T * 4);
   const int64_t o_li = off; off += al(7 * T * 4);
   const int64_t o_cnt = off; off += al(C_NCOUNTERS * 4);
   const int64_t o_fl = off; off += al((int64_t)count * 8);
@@ -742,6 +777,7 @@ int pool_create(int32_t count, const int32_t* ext, void* stream, Pool** out) {
   d.r = (int32_t*)(base + o_r); d.rmask = (uint8_t*)(base + o_rm); d.reach = (uint8_t*)(base + o_rc);
   d.nbr = (int32_t*)(base + o_nbr); d.tinst = (int32_t*)(base + o_ti); d.tpar = (uint8_t*)(base + o_tp);
   d.act = (uint8_t*)(base + o_act); d.tflag = (uint16_t*)(base + o_tf); d.stamp_bfs = (uint32_t*)(base + o_sb); d.stamp_sw = (uint32_t*)(base + o_ss);
+  d.stamp_inc = (uint32_t*)(base + o_si);
   d.lists = (int32_t*)(base + o_li); d.cnt = (int32_t*)(base + o_cnt);
   d.flow = (unsigned long long*)(base + o_fl); d.geo = (InstGeo*)(base + o_geo);
   d.stats = (unsigned long long*)(base + o_st); d.err = (int32_t*)(base + o_err); d.bar = (uint32_t*)(base + o_bar);
@@ -880,6 +916,7 @@ cgc_options resolve_options(const cgc_options* o) {
   r.region_relabels = 2;
   r.stall_sweeps = 0;
   r.ctas_per_sm = 2;
+  r.relabel = 2;
   if (o) {
     if (o->local_pulses > 0) r.local_pulses = std::min(o->local_pulses, 64);
     if (o->sweeps_per_relabel > 0) r.sweeps_per_relabel = o->sweeps_per_relabel;
@@ -891,6 +928,7 @@ cgc_options resolve_options(const cgc_options* o) {
     if (o->ctas_per_sm >= 2 && o->ctas_per_sm <= 4) r.ctas_per_sm = o->ctas_per_sm;
     r.bfs_warp_min = o->bfs_warp_min > 0 ? o->bfs_warp_min : 0;
     r.exclusive = o->exclusive > 0 ? 1 : 0;
+    if (o->relabel == 1 || o->relabel == 2) r.relabel = o->relabel;
     r.learned = (o->learned == 2 || o->learned == 3) ? o->learned : (o->learned > 0 ? 1 : 0);
     r.trace_cycles = o->trace_cycles > 0 ? std::min(o->trace_cycles, 64) : 0;
   }
@@ -914,6 +952,7 @@ SolveParams solve_params(const cgc_options& o) {
   prm.limit_ns = wait_limit_ns(o);
   prm.bfs_warp_min = o.ctas_per_sm >= 3 ? o.bfs_warp_min : 0;  // kernels k_solve3w / k_solve4w
   prm.exclusive = o.exclusive ? 1 : 0;
+  prm.incremental = o.relabel == 2 ? 1 : 0;
   return prm;
 }
 
@@ -993,6 +1032,7 @@ int pool_solve_async(Pool& p, const cgc_options* opts) {
   CGC_CUDA(cudaMemsetAsync(d.bar, 0, 8, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_bfs, 0, (size_t)d.T * 4, p.stream));
   CGC_CUDA(cudaMemsetAsync(d.stamp_sw, 0, 2 * (size_t)d.T * 4, p.stream));
+  CGC_CUDA(cudaMemsetAsync(d.stamp_inc, 0, (size_t)d.T * 4, p.stream));
   if (p.ninst == 1) {
     InputPlanes ip;
     for (int k = 0; k < 8; ++k) ip.p[k] = in[k];
@@ -1094,6 +1134,7 @@ int pool_solve_wait(Pool& p) {
   }
   p.st.tiles_swept = (int64_t)stats[S_TILES_SWEPT];
   p.st.tiles_relabelled = (int64_t)stats[S_TILES_BFS];
+  p.st.tiles_checked = (int64_t)stats[S_TILES_CHECK];
   p.st.pulses = (int64_t)stats[S_PULSES];
   p.st.solve_ms = ms;
   p.st.kernel_ms = kms;

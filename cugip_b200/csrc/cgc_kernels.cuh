@@ -652,9 +652,99 @@ __device__ inline void bfs_tile(const DevPool& P, const int t, BfsShared& S, con
   }
   const int act = __syncthreads_or(has_excess && h < INF);
   if (l == 0) {
-    if (act) P.act[t] = 1;
+    P.act[t] = (uint8_t)(act ? 1 : 0);  // heights only drop in later visits: the last visit's value is final
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
   }
+  if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) queue_tile(P, P.stamp_bfs, nb, id_next, list_next, cnt_next);
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Incremental global relabel.  Heights are a valid labelling at all times
+// (h <= d, the exact distance to the sink), and h(v) == d(v) exactly when v is
+// supported: a sink-adjacent voxel at height 1 (rT > 0), or a voxel with a
+// residual edge to a supported neighbour exactly one lower.  (Along a shortest
+// path every step of a valid labelling drops by at most one, so h == d forces
+// each step to drop by exactly one down to a seed at 1.)  Right after an exact
+// relabel every finite voxel is supported; a sweep cycle can break support
+// only inside the tiles it queued (their heights and out-residuals changed)
+// and, through their face voxels, in the face neighbours of those tiles.  So
+// the invalidation pass below visits those tiles, sets every unsupported
+// voxel to INF and re-checks the neighbours of every voxel it drops; the
+// voxels it leaves finite are exact, and the tile Bellman-Ford (bfs_tile)
+// started from the tiles with dropped voxels recomputes the rest exactly.
+// The heights that come out equal the full BFS's bit for bit.
+
+// a tile's sweep stamps (both halves under exclusive sweeps) were written
+// after id c0, i.e. the tile was queued during the current sweep cycle
+__device__ __forceinline__ bool queued_since(const DevPool& P, int t, uint32_t c0, bool exclusive) {
+  const uint32_t a = __ldcg(P.stamp_sw + t);
+  const uint32_t b = exclusive ? __ldcg(P.stamp_sw + P.T + t) : 0u;
+  return (int32_t)(a - c0) > 0 || (exclusive && (int32_t)(b - c0) > 0);
+}
+
+// Seed of the invalidation pass, one thread per tile: tiles queued during the
+// cycle and their face neighbours.
+__device__ __forceinline__ void inval_queue_tile(const DevPool& P, const int t, const uint32_t c0, const bool exclusive,
+                                                 const uint32_t id0, int32_t* list0, int32_t* cnt0) {
+  bool q = false;
+  if (t < P.T) {
+    q = queued_since(P, t, c0, exclusive);
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      const int nt = __ldcg(P.nbr + d * P.T + t);
+      if (!q && nt >= 0 && CGC_IN_BOUNDS(P, nt, P.T)) q = queued_since(P, nt, c0, exclusive);
+    }
+    if (q && (__ldcg(P.tflag + t) & TF_DEAD)) q = false;  // all INF, nothing to check
+  }
+  if (q) P.stamp_bfs[t] = id0;
+  warp_append(P, q, t, list0, cnt0);
+}
+
+// One invalidation visit: drop unsupported voxels of tile t to INF until the
+// tile is stable (drops are monotone, so in-place updates are safe and the
+// result is the largest supported set); re-queue the face neighbours of
+// dropped face voxels, and list the tile once (stamp_inc) for the BFS rounds.
+__device__ inline void inval_tile(const DevPool& P, const int t, BfsShared& S, const uint32_t id_next,
+                                  int32_t* list_next, int32_t* cnt_next, const uint32_t id_bfs, int32_t* list_bfs,
+                                  int32_t* cnt_bfs) {
+  if (!CGC_IN_BOUNDS(P, t, P.T)) return;  // uniform over the block
+  const int l = threadIdx.x;
+  const int nb = l < 6 ? __ldcg(P.nbr + l * P.T + t) : -1;  // face neighbour, for the re-queue
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  const int64_t g = (int64_t)t * TV + l;
+  int h = __ldcg(P.h + g);
+  const unsigned m = __ldcg(P.rmask + g);
+  const int hi = halo_index(x, y, z);
+  S.h[0][hi] = h;
+  load_halo_heights(P, t, S.h);
+  if (l == 0) S.flags = 0;
+  __syncthreads();
+  bool dropped = false;
+  for (int it = 0; it < 1024; ++it) {  // a drop per step climbs one height: < 512 steps in a tile
+    bool drop = false;
+    if (h < INF && !((m & 64u) && h == 1)) {
+      bool sup = false;
+#pragma unroll
+      for (int d = 0; d < 6; ++d)
+        if ((m >> d) & 1u) sup = sup || S.h[0][hi + hoff(d)] == h - 1;
+      drop = !sup;
+    }
+    if (drop) {
+      h = INF;
+      S.h[0][hi] = INF;
+      dropped = true;
+    }
+    if (!__syncthreads_or(drop)) break;
+  }
+  if (dropped) {
+    P.h[g] = INF;
+    const int fb = face_bits(x, y, z);
+    if (fb) atomicOr(&S.flags, fb);
+  }
+  const int any = __syncthreads_or(dropped);
+  if (l == 0) atomicAdd(P.stats + S_TILES_CHECK, 1ull);
+  if (l == 32 && any) queue_tile(P, P.stamp_inc, t, id_bfs, list_bfs, cnt_bfs);
   if (l < 6 && ((S.flags >> l) & 1) && nb >= 0) queue_tile(P, P.stamp_bfs, nb, id_next, list_next, cnt_next);
   __syncthreads();
 }

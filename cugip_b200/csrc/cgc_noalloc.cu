@@ -60,7 +60,8 @@ constexpr int64_t kOffAct = kOffTpar + al256(kMaxTiles);
 constexpr int64_t kOffTflag = kOffAct + al256(kMaxTiles);
 constexpr int64_t kOffStampB = kOffTflag + al256(kMaxTiles * 2);
 constexpr int64_t kOffStampS = kOffStampB + al256(kMaxTiles * 4);
-constexpr int64_t kOffLists = kOffStampS + al256(kMaxTiles * 4);
+constexpr int64_t kOffStampI = kOffStampS + al256(kMaxTiles * 4);
+constexpr int64_t kOffLists = kOffStampI + al256(kMaxTiles * 4);
 constexpr int64_t kOffCnt = kOffLists + al256(7 * kMaxTiles * 4);
 constexpr int64_t kOffFlow = kOffCnt + al256(C_NCOUNTERS * 4);
 constexpr int64_t kOffGeo = kOffFlow + al256(8);
@@ -163,6 +164,7 @@ extern "C" int cgc_grid_maxflow_noalloc(int32_t X, int32_t Y, int32_t Z, const i
   P.nbr = (const int32_t*)(base + kOffNbr); P.tinst = (const int32_t*)(base + kOffTinst);
   P.tpar = base + kOffTpar; P.act = base + kOffAct; P.tflag = (uint16_t*)(base + kOffTflag);
   P.stamp_bfs = (uint32_t*)(base + kOffStampB); P.stamp_sw = (uint32_t*)(base + kOffStampS);
+  P.stamp_inc = (uint32_t*)(base + kOffStampI);
   P.lists = (int32_t*)(base + kOffLists); P.cnt = (int32_t*)(base + kOffCnt);
   P.flow = (unsigned long long*)(base + kOffFlow); P.geo = (const InstGeo*)(base + kOffGeo);
   P.stats = (unsigned long long*)(base + kOffStats); P.err = (int32_t*)(base + kOffErr);

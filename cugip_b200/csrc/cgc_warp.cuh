@@ -134,7 +134,7 @@ __device__ inline void bfs_tile_w(const DevPool& P, const int t, WarpBfsSmem& S,
   faces = __reduce_or_sync(FULL, faces);
   act = __any_sync(FULL, act);
   if (lane == 0) {
-    if (act) P.act[t] = 1;  // only ever set during a BFS (bfs_init_tile_w clears it)
+    P.act[t] = (uint8_t)(act ? 1 : 0);  // heights only drop in later visits: the last visit's value is final
     atomicAdd(P.stats + S_TILES_BFS, 1ull);
   }
   if (lane < 6 && ((faces >> lane) & 1)) {

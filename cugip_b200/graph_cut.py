@@ -60,7 +60,7 @@ class Policy:
     def __init__(self, local_pulses: int = 0, sweeps_per_relabel: int = 0, wait_limit_us: int = 0,
                  max_sweeps: int = 0, persistent: int = 0, region_relabels: int = 0, stall_sweeps: int = 0,
                  ctas_per_sm: int = 0, learned: int = 0, trace_cycles: int = 0, bfs_warp_min: int = 0,
-                 exclusive: int = 0):
+                 exclusive: int = 0, relabel: int = 0):
         self.local_pulses = local_pulses
         self.sweeps_per_relabel = sweeps_per_relabel
         self.wait_limit_us = wait_limit_us
@@ -73,6 +73,7 @@ class Policy:
         self.trace_cycles = trace_cycles
         self.bfs_warp_min = bfs_warp_min
         self.exclusive = exclusive
+        self.relabel = relabel
 
     def options(self) -> _lib.Options:
         return _lib.options(**{k: getattr(self, k) for k in _lib.OPTION_FIELDS})
@@ -84,7 +85,7 @@ class Policy:
     def __repr__(self):
         return (f"Policy(L={self.local_pulses}, R={self.region_relabels}, K={self.sweeps_per_relabel}, "
                 f"ctas={self.ctas_per_sm}, stall={self.stall_sweeps}, learned={self.learned}, "
-                f"bfsw={self.bfs_warp_min}, excl={self.exclusive})")
+                f"bfsw={self.bfs_warp_min}, excl={self.exclusive}, relabel={self.relabel})")
 
     def with_(self, **kw) -> "Policy":
         p = Policy.from_options(self.options())

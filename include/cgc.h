@@ -83,7 +83,11 @@ typedef struct cgc_options {
   int32_t exclusive;          /* persistent: 1 = every sweep visits each queued tile, except a tile that has a
                                  face neighbour of the sweep's parity queued for the same sweep (which waits one
                                  sweep); 0 = checkerboard sweeps, one parity at a time (the default) */
-  int32_t reserved[3];
+  int32_t relabel;            /* persistent: global relabels after the first of a solve, 1 = full BFS from the
+                                 sink, 2 = incremental (re-checks the tiles the last sweep cycle queued and
+                                 recomputes only the labels it invalidated; the labels equal the full BFS's);
+                                 0 = the default (2) */
+  int32_t reserved[2];
 } cgc_options;
 
 /* Per-solve statistics (filled by cgc_grid_stats). */
@@ -102,7 +106,8 @@ typedef struct cgc_stats {
   double  sweep_ms;          /* persistent solve: time in push sweeps */
   double  reach_ms;          /* persistent solve: time in the source-side reachability */
   double  sched_ms;          /* persistent solve: time in the learned scheduler (features + CNN) */
-  int64_t reserved[2];
+  int64_t tiles_checked;     /* tile visits of the incremental relabels' invalidation passes */
+  int64_t reserved[1];
 } cgc_stats;
 
 /* Kernels launched by this library on the calling process since load

@@ -61,6 +61,7 @@ struct GraphCutPolicy {
   int learned = 0;             // learned scheduler: 1 budgets + priorities, 2 budgets only
   int bfs_warp_min = 0;        // 3/4 CTAs per SM: BFS rounds with this many tiles per CTA use a warp per tile
   int exclusive = 0;           // 1: sweeps visit every queued tile without a queued face neighbour of the sweep's parity
+  int relabel = 0;             // global relabels after a solve's first: 1 full BFS, 2 incremental (0: default, 2)
   cgc_options options() const {
     cgc_options o{};
     o.struct_size = sizeof(cgc_options);
@@ -75,6 +76,7 @@ struct GraphCutPolicy {
     o.learned = learned;
     o.bfs_warp_min = bfs_warp_min;
     o.exclusive = exclusive;
+    o.relabel = relabel;
     return o;
   }
   // The autotuner's choice for a size class (cgc_autotune_lookup), if any
@@ -94,6 +96,7 @@ struct GraphCutPolicy {
     out->learned = o.learned;
     out->bfs_warp_min = o.bfs_warp_min;
     out->exclusive = o.exclusive;
+    out->relabel = o.relabel;
     return true;
   }
 };

@@ -41,6 +41,11 @@ POLICIES = {
     "excl_cta3_L1_K1": Policy(exclusive=1, ctas_per_sm=3, local_pulses=1, sweeps_per_relabel=1),
     "excl_cta4_bfsw": Policy(exclusive=1, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
     "excl_stall": Policy(exclusive=1, stall_sweeps=1, sweeps_per_relabel=64),
+    # every global relabel a full BFS from the sink (the default re-checks
+    # only what the last sweep cycle touched)
+    "full_relabel": Policy(relabel=1),
+    "full_cta4_bfsw": Policy(relabel=1, ctas_per_sm=4, region_relabels=4, bfs_warp_min=8),
+    "full_excl_L1_K1": Policy(relabel=1, exclusive=1, local_pulses=1, sweeps_per_relabel=1),
 }
 
 
@@ -100,7 +105,7 @@ def test_long_paths_match_oracle(seed):
 
 
 @pytest.mark.parametrize("policy", ["default", "cta4_R4", "bfsw_all", "bfsw8_cta4", "cta3_L2_R4", "excl",
-                                    "excl_cta4_bfsw"])
+                                    "excl_cta4_bfsw", "full_relabel"])
 @pytest.mark.parametrize("key", [k for k in CASES if k[0] in (1, 5) or (k[0] == 4 and k[1] < 8)])
 def test_golden_workloads(key, policy):
     c = CASES[key]
@@ -112,7 +117,8 @@ def test_golden_workloads(key, policy):
     assert sha(treach) == c["treach_sha256"]
 
 
-@pytest.mark.parametrize("policy", ["default", "bfsw8_cta4", "cta3_L2_R4", "excl", "excl_cta4_bfsw"])
+@pytest.mark.parametrize("policy", ["default", "bfsw8_cta4", "cta3_L2_R4", "excl", "excl_cta4_bfsw",
+                                    "full_cta4_bfsw"])
 @pytest.mark.parametrize("key", [(2, 0), (3, 0)])
 def test_full_size_workloads_with_certificate(key, policy):
     c = CASES[key]
@@ -121,6 +127,42 @@ def test_full_size_workloads_with_certificate(key, policy):
     assert flow == c["flow"]
     assert sha(smin) == c["smin_sha256"] and sha(treach) == c["treach_sha256"]
     certify(v.X, v.Y, v.Z, v.capS, v.capT, v.n, None, flow, res, smin, treach)
+
+
+def _solve_with_labels(v, policy):
+    g = GridGraph(v.X, v.Y, v.Z)
+    try:
+        g.set_tweights(v.capS, v.capT)
+        for ax in range(3):
+            g.set_nweights(ax, v.n[ax])
+        flow = g.max_flow(policy)
+        return flow, g.labels(), g.stats(), g.fill_segments(mask=1, background=0, which=SOURCE)
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("base", ["default", "L1_K1", "cta3_L2_R4", "bfsw8_cta4", "stall3_L2", "excl",
+                                  "excl_cta3_L1_K1"])
+@pytest.mark.parametrize("key", [(1, 0), (4, 3), (4, 6), (5, 0), (2, 0), (3, 0)])
+def test_incremental_relabel_equals_full_bfs(key, base):
+    """The incremental global relabel (invalidation from the tiles a sweep
+    cycle queued, then tile Bellman-Ford from the dropped voxels) must leave
+    the full BFS's labels bit for bit.  Every later step depends only on the
+    labels, so both solves take the same sweeps, tile visits and pulses and end
+    with the same labels, flow and cuts."""
+    c = CASES[key]
+    v = volume.workload(*key)
+    pol = POLICIES[base] or Policy()
+    full = _solve_with_labels(v, pol.with_(relabel=1))
+    inc = _solve_with_labels(v, pol.with_(relabel=2))
+    assert full[0] == inc[0] == c["flow"]
+    assert np.array_equal(full[1], inc[1])
+    for k in ("sweeps", "global_relabels", "tiles_swept", "pulses"):
+        assert full[2][k] == inc[2][k], k
+    assert full[2]["tiles_checked"] == 0
+    if inc[2]["global_relabels"] > 1:
+        assert inc[2]["tiles_checked"] > 0
+    assert sha(inc[3]) == c["smin_sha256"]
 
 
 def test_batch_matches_golden():
